@@ -1,0 +1,93 @@
+// engine.cu -- template instantiations of the pair-pass kernel and the launcher.
+#include <cmath>
+
+#include "internal.h"
+
+namespace culamp_host {
+
+using namespace culamp_dev;
+
+int pmode_of(double p) {
+    if (p == 1.0) return P_L1;
+    if (p == 2.0) return P_SQ;
+    if (std::isinf(p)) return P_INF;
+    return P_GEN;
+}
+
+LaunchShape pass_shape(int n, int m, int d, int acc, int sm_count) {
+    LaunchShape s{};
+    s.rb = (n + ROWS - 1) / ROWS;
+    if (s.rb < 1) s.rb = 1;
+    const bool packed = d >= 1 && d <= MAXD_PACKED;
+    const int ch = packed ? CHUNK : CHUNK_G;
+    // Aim for ~4 resident CTAs per SM over the whole grid; never split below one tile.
+    const int target = 4 * (sm_count > 0 ? sm_count : 148);
+    int splits = (target + s.rb - 1) / s.rb;
+    const int max_splits = (m + ch - 1) / ch;
+    if (splits > max_splits) splits = max_splits;
+    if (splits < 1) splits = 1;
+    int cps = (m + splits - 1) / splits;
+    cps = ((cps + ch - 1) / ch) * ch;
+    if (cps < ch) cps = ch;
+    splits = (m + cps - 1) / cps;
+    if (splits < 1) splits = 1;
+    s.splits = splits;
+    s.cols_per_split = cps;
+    s.smem = (size_t)(packed ? CHUNK * 4 : CHUNK_G * (d + 1)) * sizeof(double);
+    s.part_bytes = splits > 1 ? (size_t)splits * (size_t)n * 3 * sizeof(double) : 0;
+    (void)acc;
+    return s;
+}
+
+template <int PM, int D, int ACC>
+static cudaError_t launch_t(const PassParams &P, const LaunchShape &sh, cudaStream_t st) {
+    auto kern = pair_pass_kernel<PM, D, ACC>;
+    if (sh.smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sh.smem);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid(sh.rb, sh.splits);
+    kern<<<grid, TPB, sh.smem, st>>>(P);
+    return cudaGetLastError();
+}
+
+template <int PM, int ACC>
+static cudaError_t launch_d(const PassParams &P, const LaunchShape &sh, cudaStream_t st) {
+    switch (P.d) {
+        case 1: return launch_t<PM, 1, ACC>(P, sh, st);
+        case 2: return launch_t<PM, 2, ACC>(P, sh, st);
+        case 3: return launch_t<PM, 3, ACC>(P, sh, st);
+        default: return launch_t<PM, 0, ACC>(P, sh, st);
+    }
+}
+
+template <int ACC>
+static cudaError_t launch_p(const PassParams &P, int pm, const LaunchShape &sh, cudaStream_t st) {
+    switch (pm) {
+        case P_L1: return launch_d<P_L1, ACC>(P, sh, st);
+        case P_SQ: return launch_d<P_SQ, ACC>(P, sh, st);
+        case P_INF: return launch_d<P_INF, ACC>(P, sh, st);
+        default: return launch_d<P_GEN, ACC>(P, sh, st);
+    }
+}
+
+cudaError_t launch_pass(PassParams P, int pm, int acc, const LaunchShape &sh, Scratch &scr,
+                        cudaStream_t st) {
+    P.splits = sh.splits;
+    P.cols_per_split = sh.cols_per_split;
+    P.part = scr.part.as<double>();
+    P.rb_ticket = scr.tickets.as<unsigned>();
+    P.grid_ticket = scr.tickets.as<unsigned>() + sh.rb;
+    P.blk = scr.blk.as<double>();
+    if (scr.part.bytes < sh.part_bytes || scr.tickets.bytes < (size_t)(sh.rb + 1) * sizeof(unsigned) ||
+        scr.blk.bytes < (size_t)sh.rb * 4 * sizeof(double))
+        return cudaErrorInvalidValue;
+    switch (acc) {
+        case ACC_LSE: return launch_p<ACC_LSE>(P, pm, sh, st);
+        case ACC_MAX: return launch_p<ACC_MAX>(P, pm, sh, st);
+        default: return launch_p<ACC_MIN>(P, pm, sh, st);
+    }
+}
+
+}  // namespace culamp_host

@@ -1,0 +1,751 @@
+// engine.cuh -- the pair-reduction tile engine of libculamp_b200 (sm_100a).
+//
+// Every hot pass of CuLAMP.jl's kernelized solvers is one reduction over all
+// (row o, column k) pairs of an on-the-fly cost C(x_o, y_k):
+//
+//   LSE_o  = log sum_k exp(alpha * C(x_o, y_k) + beta * pot_k)      (Sinkhorn / LAMP)
+//   MAX_o  = max_k C(x_o, y_k)                                       (W_inf pre-pass)
+//   MIN_o  = min_k C(x_o, y_k) + 2 W_inf theta_k                     (LAMP eta=0 dual)
+//
+// followed by a per-row epilogue (potential update, residual, LAMP mirror step)
+// and optional FP64 scalar reductions feeding the solver's convergence control.
+//
+// Design (B200):
+//  * A CTA owns ROWS = TPB*RPT output rows (RPT rows per thread, registers) and a
+//    contiguous column slice; column points + their potentials are staged through
+//    shared memory in CHUNK-column tiles (coalesced global loads, broadcast LDS).
+//  * Precision ("chosen form"): the exponent alpha*C + beta*pot is formed in FP64.
+//    For p=2 it uses C = |x|^2 + |y|^2 - 2 x.y with the column term folded into a
+//    per-column constant, so a pair costs 3 DFMA (d=3). The running row max is
+//    tracked in FP64 per KC-column sub-chunk; only the max-shifted exponent is
+//    rounded to FP32 and exponentiated on the MUFU pipe (ex2), and the sum is
+//    accumulated with compensated (Kahan) FP32 additions. Potentials, W_inf and
+//    all scalar reductions are FP64.
+//  * When one CTA row block would leave SMs idle, the column range is split over
+//    `splits` CTAs; the last CTA of a row block (atomic ticket) merges the partial
+//    (max, sum, moment) triples in a fixed order (deterministic) and runs the epilogue.
+//  * The last epilogue CTA of the grid runs the "finish" step: ordered FP64 sums of
+//    the block partials and the solver's iteration control (iteration counter,
+//    check cadence, tolerance test, itermax / tmax), so a whole solve runs from a
+//    CUDA graph with no host synchronisation per iteration.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "../../include/culamp.h"
+
+namespace culamp_dev {
+
+constexpr int TPB = 128;          // threads per CTA
+constexpr int RPT = 2;            // output rows per thread
+constexpr int ROWS = TPB * RPT;   // output rows per CTA
+constexpr int CHUNK = 256;        // columns per shared-memory tile (d <= 3)
+constexpr int KC = 4;             // columns per online-max sub-chunk
+constexpr int MAXD_PACKED = 3;    // packed fast path: d <= 3
+constexpr int MAXD = 64;          // generic path: d <= 64
+constexpr int CHUNK_G = 32;       // columns per tile on the generic path
+constexpr double LOG2E = 1.4426950408889634074;
+constexpr double LN2 = 0.69314718055994530942;
+
+enum PMode { P_L1 = 0, P_SQ = 1, P_INF = 2, P_GEN = 3 };
+enum Acc { ACC_LSE = 0, ACC_MAX = 1, ACC_MIN = 2 };
+
+// How alpha / beta of the exponent are obtained at kernel entry.
+enum CoefMode {
+    COEF_FIXED = 0,      // alpha, beta given by value
+    COEF_SK = 1,         // alpha = -1/(ctl.eta * ctl.winf), beta = 1
+    COEF_SPP_CUR = 2,    // eta_t, s = ctl.eta_t, ctl.s_t: alpha = -s/(2 W eta_t), beta = -1/eta_t
+    COEF_SPP_NEXT = 3,   // same with ctl.eta_next, ctl.s_next
+    COEF_SPP_DUAL = 4,   // reg = ctl.eta_lamp, s = 1
+};
+
+// Per-row epilogues.
+enum Epi {
+    EPI_SK_ROW = 0,      // out = log(marg) - L                          (a1)
+    EPI_SK_RESID = 1,    // res = marg - exp(rowpot + L); cost = mass*E[C] (a3)
+    EPI_LOGZ = 2,        // out = L; aux = log(marg) - L (if marg)       (a7)
+    EPI_SPP_COL = 3,     // res = exp(-rowpot/eta_t + L); cost = res*E[C] (a8) [+ LAMP step]
+    EPI_RAW = 4,         // out = value (max / min reductions)            (a6, a9)
+};
+
+enum LampStep { LAMP_NONE = 0, LAMP_A = 1, LAMP_B = 2 };
+
+enum Finish {
+    FIN_NONE = 0,
+    FIN_SUMS = 1,        // just store the ordered scalar sums into ctl->sums
+    FIN_SK_ITER = 2,     // Sinkhorn column pass: iteration bookkeeping
+    FIN_SK_CHECK = 3,    // Sinkhorn residual pass: tolerance test
+    FIN_LAMP_Z = 4,      // LAMP logZ(nu) pass: sum r.logZ
+    FIN_LAMP_A = 5,      // LAMP column pass after infeas(nu)
+    FIN_LAMP_DUAL = 6,   // LAMP dual pass: primal/dual, log, tolerance test
+    FIN_LAMP_B = 7,      // LAMP column pass after infeas(nu_bar): commit eta_t, iteration
+    FIN_MAXCOST = 8,     // W_inf = max of row maxima into ctl->winf
+};
+
+// Gate: when the kernel runs.
+enum Gate { GATE_ALWAYS = 0, GATE_CHECK = 1 };
+
+// Device-resident solver state. All fields written by device code are read by
+// later kernels only (stream order), never by concurrently running CTAs.
+struct Ctl {
+    long long iter;             // completed iterations
+    long long itermax;
+    long long frequency;
+    long long num_iter;         // the reference's num_iter counter
+    int stop;                   // kernels return immediately when set
+    int stop_reason;            // 1 tolerance, 2 itermax, 3 tmax
+    int do_check;               // the current iteration runs the check pass(es)
+    int check_enabled;          // LAMP: verbose || CHECK_ALWAYS
+    int marginal_only;          // LAMP: tolerance test ignores the gap
+    int pending_stop;           // stop after this iteration's check (itermax/tmax)
+    unsigned long long t_start_ns;
+    double tmax_s;
+    double epsilon;
+    double eta;                 // Sinkhorn eta_p of the current stage
+    double winf;
+    double residual, objective, dualval;
+    // LAMP
+    double eta_lamp;            // eta = eta_p / (2 W_inf)
+    double eta_t, s_t, eta_next, s_next, tau_p;
+    double hr;                  // eta * sum(r log r)
+    double sum_r_logz, sum_res_c, sum_cost, sum_res_nu, sum_r_dual, sum_c_theta;
+    double primal, dual;
+    // convergence log (device buffer)
+    long long log_rows, log_cap;
+    culamp_log_row *log;
+    double sums[4];             // FIN_SUMS output
+    int error;                  // device-side error code (bounded waits etc.)
+};
+
+struct PassParams {
+    const double *X;            // output-row points, point-major, ld = d
+    const double *Y;            // column points
+    int n, m, d;
+    double pexp;                // exponent for P_GEN
+    const double *ctr;          // centring point (d values) for the p=2 expansion; may be null
+    int epi;                    // Epi
+    int coef_mode;
+    double alpha, beta;         // COEF_FIXED
+    const double *colpot;       // beta * colpot_k enters the exponent; may be null
+    int colpot_unit;            // colpot enters with coefficient 1 (beta then scales rowpot)
+    const double *rowpot;       // per-row potential (EPI_SK_RESID: phi, EPI_SPP_COL: theta/nu)
+    const double *marg;         // row marginal (EPI_SK_ROW / EPI_SK_RESID / EPI_LOGZ aux)
+    double *out;                // EPI_SK_ROW / EPI_LOGZ / EPI_RAW / EPI_SPP_COL res / EPI_SK_RESID res
+    double *out2;               // cost output (may be null)
+    double *aux;                // EPI_LOGZ: log(marg) - L (may be null); EPI_SK_ROW: previous value backup
+    double minmax_scale;        // ACC_MIN: multiplier of colpot (2 W_inf)
+    // LAMP step fused into EPI_SPP_COL
+    int lamp_step;
+    double *theta, *thetab, *nu, *nub;
+    const double *cvec, *eta_mu_i;
+    double eta_mu_exp, minv, maxv;
+    // moments
+    int want_moment;            // 0 never, 1 always, 2 when ctl->do_check
+    // gating and control
+    int gate;
+    int finish;
+    Ctl *ctl;
+    // split-column scratch
+    int splits;
+    int cols_per_split;
+    double *part;               // [splits][n][3] (max, sum, moment)
+    unsigned int *rb_ticket;    // [row blocks]
+    unsigned int *grid_ticket;  // [1]
+    double *blk;                // [row blocks][4] block partial scalars
+};
+
+// 2^x on the MUFU pipe (PTX ex2.approx.ftz.f32: relative error ~2^-22, results
+// below 2^-126 flush to zero -- negligible next to the max-shifted term 1).
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Exponent coefficients (natural-log units) for this launch.
+__device__ __forceinline__ void resolve_coefs(const PassParams &P, double &alpha, double &beta) {
+    const Ctl *c = P.ctl;
+    switch (P.coef_mode) {
+        case COEF_SK:
+            alpha = -1.0 / (c->eta * c->winf);
+            beta = 1.0;
+            break;
+        case COEF_SPP_CUR:
+        case COEF_SPP_NEXT:
+        case COEF_SPP_DUAL: {
+            double et, st;
+            if (P.coef_mode == COEF_SPP_CUR) { et = c->eta_t; st = c->s_t; }
+            else if (P.coef_mode == COEF_SPP_NEXT) { et = c->eta_next; st = c->s_next; }
+            else { et = c->eta_lamp; st = 1.0; }
+            const double c1 = st / (2.0 * c->winf);
+            const double invreg = 1.0 / et;
+            alpha = -c1 * invreg;
+            beta = -invreg;
+            break;
+        }
+        default:
+            alpha = P.alpha;
+            beta = P.beta;
+    }
+}
+
+template <int PM>
+__device__ __forceinline__ double pair_cost_direct(const double *xr, const double *yk, int d, double pexp) {
+    double acc = 0.0;
+    if (PM == P_L1) {
+        for (int k = 0; k < d; ++k) acc += fabs(xr[k] - yk[k]);
+    } else if (PM == P_SQ) {
+        for (int k = 0; k < d; ++k) { double t = xr[k] - yk[k]; acc = fma(t, t, acc); }
+    } else if (PM == P_INF) {
+        for (int k = 0; k < d; ++k) acc = fmax(acc, fabs(xr[k] - yk[k]));
+    } else {
+        for (int k = 0; k < d; ++k) acc += pow(fabs(xr[k] - yk[k]), pexp);
+    }
+    return acc;
+}
+
+// Kahan-compensated FP32 accumulation of exp terms.
+struct KSum {
+    float s, c;
+    __device__ __forceinline__ void add(float v) {
+        float y = v - c;
+        float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ void scale(float f) { s *= f; c *= f; }
+};
+
+// ---------------------------------------------------------------------------
+// Main tile loop. D > 0: packed compile-time dimension (<= 3); D == 0: generic.
+// Produces per-row (M, S, MOM): LSE2 = M + log2(S) in log2 units of the shifted
+// exponent, or the max/min value in M for ACC_MAX/ACC_MIN.
+template <int PM, int D, int ACC, bool MOM>
+__device__ __forceinline__ void tile_reduce(const PassParams &P, double alpha, double beta,
+                                            int row_base, int cbeg, int cend, double *smem,
+                                            double (&Mo)[RPT], double (&So)[RPT],
+                                            double (&MOMo)[RPT], double (&Ho)[RPT]) {
+    const int tid = threadIdx.x;
+    const int d = (D > 0) ? D : P.d;
+    const bool expand = (ACC == ACC_LSE) && (PM == P_SQ);
+    const double a2 = alpha * LOG2E;          // log2-scaled cost multiplier
+    const double b2 = beta * LOG2E;
+    const int CH = (D > 0) ? CHUNK : CHUNK_G;
+    const int LD = (D > 0) ? 4 : (P.d + 1);   // doubles per staged column
+
+    double ctr[(D > 0) ? D : 1];
+    if (D > 0) {
+#pragma unroll
+        for (int k = 0; k < (D > 0 ? D : 1); ++k) ctr[k] = P.ctr ? P.ctr[k] : 0.0;
+    }
+
+    // row state
+    double xs[RPT][(D > 0) ? D : 1];          // centred row point (packed path)
+    double xt[RPT][(D > 0) ? D : 1];          // -2 a2 (x - ctr) for the p=2 expansion
+    int rows[RPT];
+    bool rvalid[RPT];
+    double M[RPT];
+    KSum S[RPT];
+    float MOMs[RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        rows[r] = row_base + tid + r * TPB;
+        rvalid[r] = rows[r] < P.n;
+        M[r] = (ACC == ACC_MIN) ? INFINITY : -INFINITY;
+        S[r].s = 0.f; S[r].c = 0.f;
+        MOMs[r] = 0.f;
+        Ho[r] = 0.0;
+        if (D > 0) {
+            double h = 0.0;
+#pragma unroll
+            for (int k = 0; k < (D > 0 ? D : 1); ++k) {
+                double v = rvalid[r] ? (P.X[(size_t)rows[r] * D + k] - ctr[k]) : 0.0;
+                xs[r][k] = v;
+                xt[r][k] = -2.0 * a2 * v;
+                h = fma(v, v, h);
+            }
+            Ho[r] = expand ? a2 * h : 0.0;
+        }
+    }
+
+    for (int c0 = cbeg; c0 < cend; c0 += CH) {
+        __syncthreads();
+        // stage CH columns: (y - ctr)[d], g
+        for (int q = tid; q < CH; q += TPB) {
+            const int j = c0 + q;
+            double *dst = smem + (size_t)q * LD;
+            const bool ok = j < cend;
+            double g;
+            if (D > 0) {
+                double yy = 0.0;
+#pragma unroll
+                for (int k = 0; k < (D > 0 ? D : 1); ++k) {
+                    double v = ok ? (P.Y[(size_t)j * D + k] - ctr[k]) : 0.0;
+                    dst[k] = v;
+                    yy = fma(v, v, yy);
+                }
+#pragma unroll
+                for (int k = (D > 0 ? D : 1); k < 3; ++k) dst[k] = 0.0;
+                double pot = (ok && P.colpot) ? P.colpot[j] : 0.0;
+                if (ACC == ACC_LSE) {
+                    const double cb = P.colpot_unit ? LOG2E : b2;
+                    g = (cb == 0.0) ? 0.0 : cb * pot;             // beta = 0 tolerates infinite pots
+                    if (expand) g += a2 * yy;
+                    if (!ok) g = -INFINITY;
+                } else if (ACC == ACC_MIN) {
+                    g = ok ? P.minmax_scale * pot : INFINITY;
+                } else {
+                    g = ok ? 0.0 : -INFINITY;
+                }
+                dst[3] = g;
+            } else {
+                for (int k = 0; k < d; ++k) dst[k] = ok ? P.Y[(size_t)j * d + k] : 0.0;
+                double pot = (ok && P.colpot) ? P.colpot[j] : 0.0;
+                const double cb = P.colpot_unit ? LOG2E : b2;
+                if (ACC == ACC_LSE) g = ok ? ((cb == 0.0) ? 0.0 : cb * pot) : -INFINITY;
+                else if (ACC == ACC_MIN) g = ok ? P.minmax_scale * pot : INFINITY;
+                else g = ok ? 0.0 : -INFINITY;
+                dst[d] = g;
+            }
+        }
+        __syncthreads();
+        const int ncols = min(CH, cend - c0);
+        const int nsub = (ncols + KC - 1) / KC;
+        for (int sc = 0; sc < nsub; ++sc) {
+            double t[RPT][KC];
+            float cst[RPT][KC];
+#pragma unroll
+            for (int kk = 0; kk < KC; ++kk) {
+                const int q = sc * KC + kk;   // q < CH always (CH % KC == 0); padded cols carry g = +-inf
+                const double *col = smem + (size_t)q * LD;
+                if (D > 0) {
+                    const double g = col[3];
+                    double yv[(D > 0) ? D : 1];
+#pragma unroll
+                    for (int k = 0; k < (D > 0 ? D : 1); ++k) yv[k] = col[k];
+#pragma unroll
+                    for (int r = 0; r < RPT; ++r) {
+                        double v;
+                        float cf = 0.f;
+                        if (expand) {
+                            v = g;
+#pragma unroll
+                            for (int k = 0; k < (D > 0 ? D : 1); ++k) v = fma(xt[r][k], yv[k], v);
+                            if (MOM) {
+                                double cc = 0.0;
+#pragma unroll
+                                for (int k = 0; k < (D > 0 ? D : 1); ++k) { double df = xs[r][k] - yv[k]; cc = fma(df, df, cc); }
+                                cf = (float)cc;
+                            }
+                        } else {
+                            const double cc = pair_cost_direct<PM>(xs[r], yv, D, P.pexp);
+                            if (ACC == ACC_LSE) v = fma(cc, a2, g);
+                            else if (ACC == ACC_MIN) v = cc + g;
+                            else v = cc + g;   // g = 0 or -inf (padding)
+                            cf = (float)cc;
+                        }
+                        t[r][kk] = v;
+                        cst[r][kk] = cf;
+                    }
+                } else {
+                    const double g = col[d];
+#pragma unroll
+                    for (int r = 0; r < RPT; ++r) {
+                        double v, cc = 0.0;
+                        if (rvalid[r]) {
+                            const double *xr = P.X + (size_t)rows[r] * d;
+                            double acc = 0.0;
+                            for (int k = 0; k < d; ++k) {
+                                double df = xr[k] - col[k];
+                                if (PM == P_L1) acc += fabs(df);
+                                else if (PM == P_SQ) acc = fma(df, df, acc);
+                                else if (PM == P_INF) acc = fmax(acc, fabs(df));
+                                else acc += pow(fabs(df), P.pexp);
+                            }
+                            cc = acc;
+                        }
+                        if (ACC == ACC_LSE) v = fma(cc, a2, g);
+                        else v = cc + g;
+                        t[r][kk] = v;
+                        cst[r][kk] = (float)cc;
+                    }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                if (ACC == ACC_LSE) {
+                    double cm = t[r][0];
+#pragma unroll
+                    for (int kk = 1; kk < KC; ++kk) cm = fmax(cm, t[r][kk]);
+                    if (cm == -INFINITY || cm != cm) continue;
+                    if (cm > M[r]) {
+                        const float f = ex2_approx((float)(M[r] - cm));
+                        S[r].scale(f);
+                        if (MOM) MOMs[r] *= f;
+                        M[r] = cm;
+                    }
+#pragma unroll
+                    for (int kk = 0; kk < KC; ++kk) {
+                        const float e = ex2_approx((float)(t[r][kk] - M[r]));
+                        S[r].add(e);
+                        if (MOM) MOMs[r] = fmaf(e, cst[r][kk], MOMs[r]);
+                    }
+                } else if (ACC == ACC_MAX) {
+#pragma unroll
+                    for (int kk = 0; kk < KC; ++kk) M[r] = fmax(M[r], t[r][kk]);
+                } else {
+#pragma unroll
+                    for (int kk = 0; kk < KC; ++kk) M[r] = fmin(M[r], t[r][kk]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        Mo[r] = M[r];
+        So[r] = (double)S[r].s + (double)(-S[r].c);
+        MOMo[r] = (double)MOMs[r];
+    }
+}
+
+// Merge (M, S, MOM) triples: value = 2^M * S (log2 units).
+__device__ __forceinline__ void merge_lse(double &M, double &S, double &MOM, double M2, double S2,
+                                          double MOM2) {
+    if (M2 == -INFINITY || S2 == 0.0) return;
+    if (M == -INFINITY || S == 0.0) { M = M2; S = S2; MOM = MOM2; return; }
+    if (M2 > M) {
+        const double f = exp2(M - M2);
+        S = S * f + S2;
+        MOM = MOM * f + MOM2;
+        M = M2;
+    } else {
+        const double f = exp2(M2 - M);
+        S += S2 * f;
+        MOM += MOM2 * f;
+    }
+}
+
+// tanh mirror step of update_theta_residual (MirrorProx.jl:159-180) with W_inf = 1
+// as the kernel driver calls it (MirrorProxKernel.jl:1104,1114).
+__device__ __forceinline__ double theta_step(double th0, double res, double c, double emu,
+                                             double eta_mu_exp, int adjust, double minv,
+                                             double maxv, double winf) {
+    const double difference = 2.0 * winf * (res - c) / emu;
+    const double maxval = fmax(difference, -difference);
+    const double expv = exp(difference - maxval) * pow((th0 + 1.0) / (1.0 - th0), 1.0 - eta_mu_exp);
+    const double em = exp(-maxval);
+    double t = (expv - em) / (expv + em);
+    if (adjust) t = fmin(fmax(t, minv), maxv);
+    return t;
+}
+
+// LAMP eta_t recursion eta_t <- 1/(tau_p + (1/eta_t)(1 - eta)) and s recursion,
+// evaluated without contraction so it matches a plain IEEE evaluation.
+__device__ __forceinline__ void lamp_next(double eta_t, double s_t, double tau_p, double eta,
+                                          double &eta_n, double &s_n) {
+    const double inv = __drcp_rn(eta_t);
+    eta_n = __ddiv_rn(1.0, __dadd_rn(tau_p, __dmul_rn(inv, __dsub_rn(1.0, eta))));
+    s_n = __dadd_rn(__dmul_rn(__dsub_rn(1.0, eta_n), s_t), eta_n);
+}
+
+__device__ __forceinline__ void put_log(Ctl *c, double it, double infeas, double obj, double primal,
+                                        double dual) {
+    if (!c->log || c->log_rows >= c->log_cap) return;
+    culamp_log_row *r = &c->log[c->log_rows++];
+    r->time_s = (double)(globaltimer_ns() - c->t_start_ns) * 1e-9;
+    r->iter = it;
+    r->infeas = infeas;
+    r->ot_objective = obj;
+    r->primal = primal;
+    r->dual = dual;
+}
+
+// Iteration bookkeeping shared by the Sinkhorn and LAMP control steps.
+__device__ __forceinline__ void end_of_iteration(Ctl *c) {
+    c->iter += 1;
+    if (c->iter >= c->itermax) c->pending_stop = 2;
+    else if ((double)(globaltimer_ns() - c->t_start_ns) * 1e-9 > c->tmax_s) c->pending_stop = 3;
+}
+
+static __device__ __noinline__ void run_finish(const PassParams &P, const double (&tot)[4]) {
+    Ctl *c = P.ctl;
+    switch (P.finish) {
+        case FIN_SUMS:
+            for (int k = 0; k < 4; ++k) c->sums[k] = tot[k];
+            break;
+        case FIN_MAXCOST:
+            c->winf = tot[0];
+            break;
+        case FIN_SK_ITER: {
+            // after the psi update of iteration it = iter + 1; tot[0] = sum c.psi
+            c->dualval = tot[0];
+            end_of_iteration(c);
+            c->do_check = ((c->iter - 1) % c->frequency) == 0;
+            if (!c->do_check && c->pending_stop) { c->stop = 1; c->stop_reason = c->pending_stop; c->num_iter += 1; }
+            else if (!c->do_check) c->num_iter += 1;
+            break;
+        }
+        case FIN_SK_CHECK: {
+            const double l1 = tot[0];
+            c->residual = l1;
+            c->objective = tot[1];
+            put_log(c, (double)c->iter, l1, tot[1], nan(""), c->dualval + tot[2]);
+            if (l1 <= c->epsilon / 6.0) { c->stop = 1; c->stop_reason = 1; }
+            else {
+                c->num_iter += 1;
+                if (c->pending_stop) { c->stop = 1; c->stop_reason = c->pending_stop; }
+            }
+            break;
+        }
+        case FIN_LAMP_Z:
+            c->sum_r_logz = tot[0];
+            break;
+        case FIN_LAMP_A: {
+            c->sum_res_c = tot[0];
+            c->sum_cost = tot[1];
+            c->sum_res_nu = tot[2];
+            double en, sn;
+            lamp_next(c->eta_t, c->s_t, c->tau_p, c->eta_lamp, en, sn);
+            c->eta_next = en;
+            c->s_next = sn;
+            break;
+        }
+        case FIN_LAMP_DUAL: {
+            // MirrorProxKernel.jl:1084-1100
+            const double q = c->eta_lamp / c->eta_t;
+            const double primal = c->sum_cost * (1.0 - q) - q * c->sum_res_nu + q * c->sum_r_logz +
+                                  2.0 * c->winf * c->sum_res_c;
+            double dual;
+            if (c->eta_lamp > 0) dual = -2.0 * c->eta_lamp * tot[0] - 2.0 * c->winf * c->sum_c_theta + 2.0 * c->hr;
+            else dual = tot[0] - 2.0 * c->winf * c->sum_c_theta;
+            c->primal = primal;
+            c->dual = dual;
+            c->residual = c->sum_res_c;
+            c->objective = c->sum_cost;
+            put_log(c, (double)(c->iter + 1), c->sum_res_c, c->sum_cost, primal, dual);
+            const bool gap_ok = c->marginal_only ? true : (primal - dual < c->epsilon / 6.0);
+            if (gap_ok && c->sum_res_c < c->epsilon / 6.0) { c->stop = 1; c->stop_reason = 1; }
+            break;
+        }
+        case FIN_LAMP_B: {
+            c->eta_t = c->eta_next;
+            c->s_t = c->s_next;
+            end_of_iteration(c);
+            c->num_iter = c->iter;
+            c->do_check = c->check_enabled && ((c->iter % c->frequency) == 0);
+            if (c->pending_stop) { c->stop = 1; c->stop_reason = c->pending_stop; }
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+// Block-wide FP64 sum of up to 4 values per thread; result valid in thread 0.
+__device__ __forceinline__ void block_sum4(double (&v)[4], double *red) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        v[k] = x;
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0)
+        for (int k = 0; k < 4; ++k) red[w * 4 + k] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 4; ++k) {
+            double s = 0.0;
+            for (int ww = 0; ww < TPB / 32; ++ww) s += red[ww * 4 + k];
+            v[k] = s;
+        }
+    }
+}
+
+
+// Block-wide FP64 max of one value; result valid in thread 0.
+__device__ __forceinline__ double block_max1(double x, double *red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_down_sync(0xffffffffu, x, o));
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) red[w] = x;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int ww = 1; ww < TPB / 32; ++ww) x = fmax(x, red[ww]);
+    return x;
+}
+
+template <int PM, int D, int ACC>
+__global__ void __launch_bounds__(TPB) pair_pass_kernel(PassParams P) {
+    extern __shared__ __align__(16) double smem[];
+    __shared__ double red[4 * (TPB / 32)];
+    __shared__ int s_last;
+    Ctl *ctl = P.ctl;
+    if (ctl) {
+        if (ctl->stop) return;
+        if (P.gate == GATE_CHECK && !ctl->do_check) return;
+    }
+    double alpha = 0.0, beta = 0.0;
+    if (ACC == ACC_LSE) resolve_coefs(P, alpha, beta);
+    const bool mom = (P.want_moment == 1) || (P.want_moment == 2 && ctl && ctl->do_check);
+
+    const int rb = blockIdx.x;               // row block
+    const int sp = blockIdx.y;               // column split
+    const int row_base = rb * ROWS;
+    const int cbeg = sp * P.cols_per_split;
+    const int cend = min(P.m, cbeg + P.cols_per_split);
+
+    double Mv[RPT], Sv[RPT], MOMv[RPT], Hv[RPT];
+    if (ACC == ACC_LSE && mom)
+        tile_reduce<PM, D, ACC, true>(P, alpha, beta, row_base, cbeg, cend, smem, Mv, Sv, MOMv, Hv);
+    else
+        tile_reduce<PM, D, ACC, false>(P, alpha, beta, row_base, cbeg, cend, smem, Mv, Sv, MOMv, Hv);
+
+    if (P.splits > 1) {
+        // publish partials, take a ticket; the last CTA of this row block merges
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int row = row_base + threadIdx.x + r * TPB;
+            if (row < P.n) {
+                double *pp = P.part + ((size_t)sp * P.n + row) * 3;
+                pp[0] = Mv[r]; pp[1] = Sv[r]; pp[2] = MOMv[r];
+            }
+        }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned t = atomicAdd(&P.rb_ticket[rb], 1u);
+            s_last = (t == (unsigned)(P.splits - 1));
+        }
+        __syncthreads();
+        if (!s_last) return;
+        __threadfence();
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int row = row_base + threadIdx.x + r * TPB;
+            if (row >= P.n) continue;
+            double M = (ACC == ACC_MIN) ? INFINITY : -INFINITY, S = 0.0, MO = 0.0;
+            for (int s2 = 0; s2 < P.splits; ++s2) {
+                const volatile double *pp = P.part + ((size_t)s2 * P.n + row) * 3;
+                const double m2 = pp[0], ss2 = pp[1], mo2 = pp[2];
+                if (ACC == ACC_LSE) merge_lse(M, S, MO, m2, ss2, mo2);
+                else if (ACC == ACC_MAX) M = fmax(M, m2);
+                else M = fmin(M, m2);
+            }
+            Mv[r] = M; Sv[r] = S; MOMv[r] = MO;
+        }
+        if (threadIdx.x == 0) P.rb_ticket[rb] = 0u;   // re-arm for the next launch
+    }
+
+    // ---------------- epilogue: one thread per output row
+    double acc4[4] = {0.0, 0.0, 0.0, 0.0};
+    double amax = -INFINITY;
+    double en = 0.0;
+    if (P.lamp_step == LAMP_A) { double sn; lamp_next(ctl->eta_t, ctl->s_t, ctl->tau_p, ctl->eta_lamp, en, sn); }
+    else if (P.lamp_step == LAMP_B) en = ctl->eta_next;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        const int o = row_base + threadIdx.x + r * TPB;
+        if (o >= P.n) continue;
+        if (ACC != ACC_LSE) {
+            if (P.out) P.out[o] = Mv[r];
+            amax = fmax(amax, Mv[r]);
+            if (P.marg) acc4[0] += P.marg[o] * Mv[r];
+            continue;
+        }
+        // natural-log LSE of the row: ln2 * (H + M + log2 S)
+        const double L = LN2 * (Hv[r] + Mv[r] + log2(Sv[r]));
+        const double Ec = (Sv[r] > 0.0) ? MOMv[r] / Sv[r] : 0.0;   // softmax-weighted mean cost
+        switch (P.epi) {
+            case EPI_SK_ROW: {
+                const double v = log(P.marg[o]) - L;
+                P.out[o] = v;
+                acc4[0] += P.marg[o] * v;
+                break;
+            }
+            case EPI_SK_RESID: {
+                const double mass = exp(P.rowpot[o] + L);
+                const double res = P.marg[o] - mass;
+                if (P.out) P.out[o] = res;
+                if (P.out2) P.out2[o] = mass * Ec;
+                acc4[0] += fabs(res);
+                acc4[1] += mass * Ec;
+                acc4[2] += P.marg[o] * P.rowpot[o];
+                break;
+            }
+            case EPI_LOGZ: {
+                if (P.out) P.out[o] = L;
+                if (P.marg) {
+                    if (P.aux) P.aux[o] = log(P.marg[o]) - L;
+                    acc4[0] += P.marg[o] * L;
+                }
+                break;
+            }
+            case EPI_SPP_COL: {
+                const double rp = P.rowpot ? P.rowpot[o] : 0.0;
+                const double res = exp(((beta == 0.0) ? 0.0 : beta * rp) + L);
+                const double cst = res * Ec;
+                if (P.out) P.out[o] = res;
+                if (P.out2) P.out2[o] = cst;
+                const double cj = P.cvec ? P.cvec[o] : 0.0;
+                acc4[0] += fabs(res - cj);
+                acc4[1] += cst;
+                acc4[2] += res * rp;
+                if (P.lamp_step == LAMP_A) {
+                    const double th = P.theta[o];
+                    acc4[3] += cj * th;
+                    P.thetab[o] = theta_step(th, res, cj, P.eta_mu_i[o], P.eta_mu_exp, 0, P.minv, P.maxv, 1.0);
+                    P.nub[o] = (1.0 - en) * P.nu[o] + en * th;
+                } else if (P.lamp_step == LAMP_B) {
+                    P.theta[o] = theta_step(P.theta[o], res, cj, P.eta_mu_i[o], P.eta_mu_exp, 1, P.minv, P.maxv, 1.0);
+                    P.nu[o] = (1.0 - en) * P.nu[o] + en * P.thetab[o];
+                }
+                break;
+            }
+            default:
+                if (P.out) P.out[o] = L;
+                break;
+        }
+    }
+
+    if (P.finish == FIN_NONE) return;
+    if (ACC == ACC_MAX) {
+        const double bm = block_max1(amax, red);
+        acc4[0] = bm;
+    } else {
+        block_sum4(acc4, red);
+    }
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 4; ++k) P.blk[rb * 4 + k] = acc4[k];
+        __threadfence();
+        const unsigned t = atomicAdd(P.grid_ticket, 1u);
+        s_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        __threadfence();
+        double tot[4] = {0.0, 0.0, 0.0, 0.0};
+        if (ACC == ACC_MAX) tot[0] = -INFINITY;
+        for (int b = 0; b < (int)gridDim.x; ++b) {
+            const volatile double *bb = P.blk + b * 4;
+            if (ACC == ACC_MAX) tot[0] = fmax(tot[0], bb[0]);
+            else for (int k = 0; k < 4; ++k) tot[k] += bb[k];
+        }
+        if (P.finish == FIN_LAMP_A) ctl->sum_c_theta = tot[3];
+        run_finish(P, tot);
+        *P.grid_ticket = 0u;
+    }
+}
+
+}  // namespace culamp_dev

@@ -1,0 +1,90 @@
+// internal.h -- host-side internals shared by the libculamp_b200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstddef>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/culamp.h"
+#include "engine.cuh"
+
+namespace culamp_host {
+
+using culamp_dev::Ctl;
+using culamp_dev::PassParams;
+
+// Growable device buffer owned by a handle.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t want, bool zero = false) {
+        if (want <= bytes) return cudaSuccess;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&ptr, want);
+        if (e != cudaSuccess) { ptr = nullptr; return e; }
+        bytes = want;
+        if (zero) e = cudaMemset(ptr, 0, want);
+        return e;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    template <class T> T *as() const { return reinterpret_cast<T *>(ptr); }
+};
+
+// Scratch used by one pair pass (split partials, tickets, block partials).
+struct Scratch {
+    DevBuf part;       // splits * rows * 3 doubles
+    DevBuf tickets;    // row blocks + 1 unsigned, zero-initialised, re-armed by kernels
+    DevBuf blk;        // row blocks * 4 doubles
+    cudaError_t reserve(size_t part_bytes, size_t nrb) {
+        cudaError_t e = part.reserve(part_bytes > 0 ? part_bytes : 8);
+        if (e != cudaSuccess) return e;
+        e = tickets.reserve((nrb + 1) * sizeof(unsigned), true);
+        if (e != cudaSuccess) return e;
+        return blk.reserve(nrb * 4 * sizeof(double) + 32);
+    }
+    void release() { part.release(); tickets.release(); blk.release(); }
+};
+
+struct LaunchShape {
+    int rb;            // row blocks
+    int splits;        // column splits
+    int cols_per_split;
+    size_t smem;       // dynamic shared memory bytes
+    size_t part_bytes; // split scratch bytes
+};
+
+// Grid and scratch requirement of a pass over n output rows and m columns.
+LaunchShape pass_shape(int n, int m, int d, int acc, int sm_count);
+
+// Launch one pair pass. The scratch must already hold pass_shape(...) bytes
+// (so the call is legal inside stream capture).
+cudaError_t launch_pass(PassParams P, int pmode, int acc, const LaunchShape &sh, Scratch &scr,
+                        cudaStream_t st);
+
+int pmode_of(double p);   // P_L1 / P_SQ / P_INF / P_GEN
+
+}  // namespace culamp_host
+
+// The opaque handle.
+struct culamp_handle_s {
+    int device = 0;
+    int sm_count = 148;
+    std::string err;
+    culamp_host::Scratch scratch;      // pass-level scratch
+    culamp_host::DevBuf pass_ctl;      // Ctl for pass-level / post-loop calls
+    culamp_host::DevBuf tmpA, tmpB;    // pass-level temporaries
+    struct Solver;                     // solver workspaces and cached graphs
+    Solver *solver = nullptr;
+};
+
+int culamp_set_error(culamp_handle h, int code, const char *fmt, ...);

@@ -1,0 +1,901 @@
+// solvers.cu -- chosen-form solver drivers: Sinkhorn (SinkhornKernel.jl:477-559),
+// LAMP (MirrorProxKernel.jl:1019-1132) and annealed Sinkhorn (AnnealedSinkhorn.jl:149-261).
+//
+// A solve is one CUDA graph: a conditional WHILE node whose body holds U
+// unrolled iterations (each a fixed sequence of pair passes) followed by a
+// one-thread control kernel that keeps the loop running while ctl->stop == 0.
+// Iteration counting, the check cadence, the tolerance test, itermax and tmax
+// all live in the passes' device-side "finish" steps, so the host launches the
+// graph once and synchronises once per solve (the reference synchronises after
+// every launch, SinkhornKernel.jl:525 / MirrorProxKernel.jl:1049-1117).
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <vector>
+
+#include "internal.h"
+#include "small_kernels.cuh"
+
+using namespace culamp_host;
+using namespace culamp_dev;
+
+#define CUDA_TRY(h, expr)                                                                       \
+    do {                                                                                        \
+        cudaError_t _e = (expr);                                                                \
+        if (_e != cudaSuccess)                                                                  \
+            return culamp_set_error((h), CULAMP_ERR_CUDA, "%s: %s (%s:%d)", #expr,             \
+                                    cudaGetErrorString(_e), __FILE__, __LINE__);                \
+    } while (0)
+
+int culamp_plain_sinkhorn(culamp_handle h, const double *x, const double *y, int64_t n, int64_t m,
+                          int32_t d, const double *r, const double *c, const culamp_args *args,
+                          int64_t frequency, double p, const double *phi0, const double *psi0,
+                          uint32_t flags, double *phi, double *psi, culamp_stats *stats,
+                          culamp_log_row *log, int64_t log_cap, cudaStream_t st);
+int culamp_plain_lamp(culamp_handle h, const double *x, const double *y, int64_t n, int64_t m,
+                      int32_t d, const double *r, const double *c, const culamp_args *args,
+                      int64_t frequency, double p, uint32_t flags, double *nu, double *phi,
+                      double *psi, double *theta, culamp_stats *stats, culamp_log_row *log,
+                      int64_t log_cap, cudaStream_t st);
+
+namespace culamp_dev {
+
+__global__ void set_start_kernel(Ctl *c) { c->t_start_ns = globaltimer_ns(); }
+
+// Loop control of the WHILE node. The hard bound on iter makes the loop finite
+// even if a finish step never ran (it cannot exceed itermax + 2 iterations).
+__global__ void loop_ctl_kernel(Ctl *c, cudaGraphConditionalHandle hnd) {
+    if (!c->stop && c->iter > c->itermax + 1) { c->stop = 1; c->stop_reason = 2; c->error = 1; }
+    cudaGraphSetConditional(hnd, c->stop ? 0u : 1u);
+}
+
+}  // namespace culamp_dev
+
+enum SolverKind { KIND_SK = 1, KIND_LAMP = 2 };
+
+// Everything a captured graph bakes into kernel parameters.
+struct GraphKey {
+    int kind = 0, n = 0, m = 0, d = 0, pm_iter = 0, pm_resid = 0, unroll = 0;
+    double p = 0, winf = 0, B = 0, eta_mu = 0;
+    long long generation = -1;
+    bool operator==(const GraphKey &o) const {
+        return kind == o.kind && n == o.n && m == o.m && d == o.d && pm_iter == o.pm_iter &&
+               pm_resid == o.pm_resid && unroll == o.unroll && generation == o.generation &&
+               std::memcmp(&p, &o.p, sizeof(double)) == 0 && std::memcmp(&winf, &o.winf, sizeof(double)) == 0 &&
+               std::memcmp(&B, &o.B, sizeof(double)) == 0 && std::memcmp(&eta_mu, &o.eta_mu, sizeof(double)) == 0;
+    }
+};
+
+struct culamp_handle_s::Solver {
+    int n = 0, m = 0, d = 0;
+    long long generation = 0;
+    DevBuf X, Y, r, c, phi, psi, res, cost, logz, aux, nu, nub, theta, thetab, eta_mu, tmp, ctl,
+        logbuf, setup, ws_phi, ws_psi, prev_phi, prev_psi;
+    DevBuf hx, hy;             // host-variant staging (device side)
+    Scratch scr;
+    cudaStream_t cap_stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    struct Cached { GraphKey key; cudaGraphExec_t exec = nullptr; };
+    std::vector<Cached> graphs;
+
+    void drop_graphs() {
+        for (auto &g : graphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+    }
+    void release() {
+        drop_graphs();
+        DevBuf *all[] = {&X, &Y, &r, &c, &phi, &psi, &res, &cost, &logz, &aux, &nu, &nub, &theta,
+                         &thetab, &eta_mu, &tmp, &ctl, &logbuf, &setup, &ws_phi, &ws_psi,
+                         &prev_phi, &prev_psi, &hx, &hy};
+        for (DevBuf *b : all) b->release();
+        scr.release();
+        if (cap_stream) cudaStreamDestroy(cap_stream);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        cap_stream = nullptr;
+        ev0 = ev1 = nullptr;
+    }
+};
+
+void culamp_solver_release(culamp_handle h) {
+    if (h && h->solver) {
+        h->solver->release();
+        delete h->solver;
+        h->solver = nullptr;
+    }
+}
+
+namespace {
+
+using Solver = culamp_handle_s::Solver;
+
+int ensure_solver(culamp_handle h, int n, int m, int d, int64_t log_cap) {
+    if (!h->solver) {
+        h->solver = new (std::nothrow) Solver();
+        if (!h->solver) return culamp_set_error(h, CULAMP_ERR_ALLOC, "solver state");
+        if (cudaStreamCreateWithFlags(&h->solver->cap_stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreate(&h->solver->ev0) != cudaSuccess || cudaEventCreate(&h->solver->ev1) != cudaSuccess)
+            return culamp_set_error(h, CULAMP_ERR_CUDA, "stream/event creation failed");
+    }
+    Solver &S = *h->solver;
+    const size_t nm = (size_t)(n > m ? n : m);
+    auto ptrs = [&S]() {
+        return std::vector<void *>{S.X.ptr, S.Y.ptr, S.r.ptr, S.c.ptr, S.phi.ptr, S.psi.ptr,
+                                   S.res.ptr, S.cost.ptr, S.logz.ptr, S.aux.ptr, S.nu.ptr,
+                                   S.nub.ptr, S.theta.ptr, S.thetab.ptr, S.eta_mu.ptr, S.tmp.ptr,
+                                   S.ctl.ptr, S.logbuf.ptr, S.scr.part.ptr, S.scr.tickets.ptr,
+                                   S.scr.blk.ptr};
+    };
+    const std::vector<void *> before = ptrs();
+    cudaError_t e = cudaSuccess;
+    auto R = [&](DevBuf &b, size_t bytes, bool zero = false) {
+        if (e == cudaSuccess) e = b.reserve(bytes, zero);
+    };
+    R(S.X, (size_t)n * d * sizeof(double));
+    R(S.Y, (size_t)m * d * sizeof(double));
+    R(S.r, nm * sizeof(double));
+    R(S.c, nm * sizeof(double));
+    R(S.phi, nm * sizeof(double));
+    R(S.psi, nm * sizeof(double));
+    R(S.res, nm * sizeof(double));
+    R(S.cost, nm * sizeof(double));
+    R(S.logz, nm * sizeof(double));
+    R(S.aux, nm * sizeof(double));
+    R(S.nu, nm * sizeof(double));
+    R(S.nub, nm * sizeof(double));
+    R(S.theta, nm * sizeof(double));
+    R(S.thetab, nm * sizeof(double));
+    R(S.eta_mu, nm * sizeof(double));
+    R(S.tmp, nm * sizeof(double));
+    R(S.ws_phi, nm * sizeof(double));
+    R(S.ws_psi, nm * sizeof(double));
+    R(S.prev_phi, nm * sizeof(double));
+    R(S.prev_psi, nm * sizeof(double));
+    R(S.ctl, sizeof(Ctl), true);
+    R(S.setup, 8 * sizeof(double));
+    R(S.logbuf, (size_t)(log_cap > 1 ? log_cap : 1) * sizeof(culamp_log_row));
+    // scratch for both pass orientations
+    LaunchShape a = pass_shape(n, m, d, ACC_LSE, h->sm_count);
+    LaunchShape b = pass_shape(m, n, d, ACC_LSE, h->sm_count);
+    const size_t pb = a.part_bytes > b.part_bytes ? a.part_bytes : b.part_bytes;
+    const size_t nrb = (size_t)(a.rb > b.rb ? a.rb : b.rb);
+    if (e == cudaSuccess) e = S.scr.reserve(pb, nrb);
+    if (e != cudaSuccess) return culamp_set_error(h, CULAMP_ERR_ALLOC, "workspace: %s", cudaGetErrorString(e));
+    if (before != ptrs()) {   // any pointer baked into a cached graph moved
+        S.generation++;
+        S.drop_graphs();
+    }
+    S.n = n;
+    S.m = m;
+    S.d = d;
+    return CULAMP_OK;
+}
+
+// Iterations per graph body: about 200 us of work per body.
+int pick_unroll(double pairs_per_iter) {
+    const double t_us = pairs_per_iter / 1.0e6 + 6.0;   // ~1e12 pairs/s + launch gaps
+    int u = (int)std::ceil(200.0 / t_us);
+    if (u < 1) u = 1;
+    if (u > 16) u = 16;
+    return u;
+}
+
+// Build (or fetch) a WHILE graph whose body runs `body` `unroll` times.
+int get_graph(culamp_handle h, const GraphKey &key, const std::function<cudaError_t(cudaStream_t)> &body,
+              cudaGraphExec_t *out) {
+    Solver &S = *h->solver;
+    for (auto &g : S.graphs)
+        if (g.key == key) { *out = g.exec; return CULAMP_OK; }
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(h, cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle ch;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&ch, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams np = {};
+    cudaGraphNode_t node;
+    if (e == cudaSuccess) {
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = ch;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+    }
+    if (e == cudaSuccess) {
+        cudaGraph_t bodyg = np.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(S.cap_stream, bodyg, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            cudaError_t eb = cudaSuccess;
+            for (int u = 0; u < key.unroll && eb == cudaSuccess; ++u) eb = body(S.cap_stream);
+            if (eb == cudaSuccess) {
+                loop_ctl_kernel<<<1, 1, 0, S.cap_stream>>>(S.ctl.as<Ctl>(), ch);
+                eb = cudaGetLastError();
+            }
+            cudaGraph_t captured = nullptr;
+            e = cudaStreamEndCapture(S.cap_stream, &captured);
+            if (eb != cudaSuccess) e = eb;
+        }
+    }
+    cudaGraphExec_t exec = nullptr;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return culamp_set_error(h, CULAMP_ERR_CUDA, "graph build: %s", cudaGetErrorString(e));
+    }
+    if (S.graphs.size() > 8) S.drop_graphs();
+    S.graphs.push_back({key, exec});
+    *out = exec;
+    return CULAMP_OK;
+}
+
+int check_solver_args(culamp_handle h, const double *x, const double *y, int64_t n, int64_t m,
+                      int32_t d, const double *r, const double *c, const culamp_args *args,
+                      int64_t frequency, double p) {
+    if (!h) return CULAMP_ERR_INVALID_ARG;
+    if (!x || !y || !r || !c || !args)
+        return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "null pointer argument");
+    if (n < 1 || m < 1 || n > (1LL << 28) || m > (1LL << 28))
+        return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "sizes out of range (n=%lld, m=%lld)",
+                                (long long)n, (long long)m);
+    if (d < 1 || d > MAXD)
+        return culamp_set_error(h, d < 1 ? CULAMP_ERR_INVALID_ARG : CULAMP_ERR_UNSUPPORTED,
+                                "d=%d outside [1, %d]", d, MAXD);
+    if (!(p > 0.0)) return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "p must be > 0");
+    if (frequency < 1) return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "frequency must be >= 1");
+    if (args->itermax < 0) return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "itermax < 0");
+    cudaSetDevice(h->device);
+    return CULAMP_OK;
+}
+
+// Copy user inputs into the workspace, validate marginals (positive, finite).
+int stage_inputs(culamp_handle h, const double *x, const double *y, int n, int m, int d,
+                 const double *r, const double *c, cudaStream_t st, double *hr_out) {
+    Solver &S = *h->solver;
+    CUDA_TRY(h, cudaMemcpyAsync(S.X.ptr, x, (size_t)n * d * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemcpyAsync(S.Y.ptr, y, (size_t)m * d * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemcpyAsync(S.r.ptr, r, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemcpyAsync(S.c.ptr, c, (size_t)m * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    double *su = S.setup.as<double>();
+    setup_reduce_kernel<<<1, 256, 0, st>>>(su, S.r.as<double>(), n);
+    setup_reduce_kernel<<<1, 256, 0, st>>>(su + 3, S.c.as<double>(), m);
+    CUDA_TRY(h, cudaGetLastError());
+    double hv[6];
+    CUDA_TRY(h, cudaMemcpyAsync(hv, su, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    if (!(hv[1] > 0.0) || !(hv[4] > 0.0) || !std::isfinite(hv[2]) || !std::isfinite(hv[5]))
+        return culamp_set_error(h, CULAMP_ERR_INVALID_ARG,
+                                "marginals must be positive and finite (min r=%g, min c=%g)", hv[1], hv[4]);
+    if (hr_out) *hr_out = hv[0];
+    return CULAMP_OK;
+}
+
+PassParams mk(const double *X, const double *Y, int n, int m, int d, double p, Ctl *ctl) {
+    PassParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.X = X;
+    P.Y = Y;
+    P.n = n;
+    P.m = m;
+    P.d = d;
+    P.pexp = p;
+    P.ctl = ctl;
+    return P;
+}
+
+// W_inf = max_ij C_ij with the solver's true p (MirrorProxKernel.jl:280-326).
+int compute_winf(culamp_handle h, int n, int m, int d, double p, cudaStream_t st, double *winf) {
+    Solver &S = *h->solver;
+    PassParams P = mk(S.X.as<double>(), S.Y.as<double>(), n, m, d, p, h->pass_ctl.as<Ctl>());
+    P.epi = EPI_RAW;
+    P.finish = FIN_MAXCOST;
+    LaunchShape sh = pass_shape(n, m, d, ACC_MAX, h->sm_count);
+    CUDA_TRY(h, launch_pass(P, pmode_of(p), ACC_MAX, sh, S.scr, st));
+    CUDA_TRY(h, cudaMemcpyAsync(winf, &h->pass_ctl.as<Ctl>()->winf, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    return CULAMP_OK;
+}
+
+void fill_stats_common(culamp_stats *stats, const Ctl &c, float ms) {
+    stats->iterations = c.iter;
+    stats->num_iter = c.num_iter;
+    stats->stopped = c.stop_reason;
+    stats->elapsed_ms = ms;
+    stats->log_rows = c.log_rows;
+    stats->status = c.error ? CULAMP_ERR_DEVICE_TIMEOUT : CULAMP_OK;
+}
+
+int copy_log(culamp_handle h, const Ctl &c, culamp_log_row *log, int64_t log_cap, cudaStream_t st) {
+    if (!log || log_cap <= 0 || c.log_rows <= 0) return CULAMP_OK;
+    const long long rows = c.log_rows < log_cap ? c.log_rows : log_cap;
+    CUDA_TRY(h, cudaMemcpyAsync(log, h->solver->logbuf.ptr, (size_t)rows * sizeof(culamp_log_row),
+                                cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    return CULAMP_OK;
+}
+
+// ------------------------------------------------------------------ Sinkhorn
+
+struct SkPlan {
+    PassParams k1, k2, k3;
+    int pm_iter, pm_resid;
+    LaunchShape s_rows, s_cols;
+};
+
+SkPlan make_sk_plan(culamp_handle h, int n, int m, int d, double p, uint32_t flags) {
+    Solver &S = *h->solver;
+    Ctl *ctl = S.ctl.as<Ctl>();
+    SkPlan pl;
+    const bool true_pinf = flags & CULAMP_FLAG_TRUE_PINF;
+    // SinkhornKernel.jl:518-523 (iteration cost), :38-42 (residual cost)
+    const double p_iter = (std::isinf(p) && !true_pinf) ? 2.0 : p;
+    const double p_res = true_pinf ? p : (p == 1.0 ? 1.0 : 2.0);
+    pl.pm_iter = pmode_of(p_iter);
+    pl.pm_resid = pmode_of(p_res);
+    double *X = S.X.as<double>(), *Y = S.Y.as<double>();
+    // K1: phi = log r - LSE_j(-C/(eta W) + psi)
+    pl.k1 = mk(X, Y, n, m, d, p_iter, ctl);
+    pl.k1.ctr = X;
+    pl.k1.epi = EPI_SK_ROW;
+    pl.k1.coef_mode = COEF_SK;
+    pl.k1.colpot = S.psi.as<double>();
+    pl.k1.marg = S.r.as<double>();
+    pl.k1.out = S.phi.as<double>();
+    // K2: psi = log c - LSE_i(-C/(eta W) + phi); iteration bookkeeping
+    pl.k2 = mk(Y, X, m, n, d, p_iter, ctl);
+    pl.k2.ctr = X;
+    pl.k2.epi = EPI_SK_ROW;
+    pl.k2.coef_mode = COEF_SK;
+    pl.k2.colpot = S.phi.as<double>();
+    pl.k2.marg = S.c.as<double>();
+    pl.k2.out = S.psi.as<double>();
+    pl.k2.finish = FIN_SK_ITER;
+    // K3 (check iterations): row residual + transport cost, tolerance test
+    pl.k3 = mk(X, Y, n, m, d, p_res, ctl);
+    pl.k3.ctr = X;
+    pl.k3.epi = EPI_SK_RESID;
+    pl.k3.coef_mode = COEF_SK;
+    pl.k3.colpot = S.psi.as<double>();
+    pl.k3.rowpot = S.phi.as<double>();
+    pl.k3.marg = S.r.as<double>();
+    pl.k3.out = S.res.as<double>();
+    pl.k3.out2 = S.cost.as<double>();
+    pl.k3.want_moment = 1;
+    pl.k3.gate = GATE_CHECK;
+    pl.k3.finish = FIN_SK_CHECK;
+    pl.s_rows = pass_shape(n, m, d, ACC_LSE, h->sm_count);
+    pl.s_cols = pass_shape(m, n, d, ACC_LSE, h->sm_count);
+    return pl;
+}
+
+// Runs the Sinkhorn loop on the workspace (phi/psi hold the starting point).
+int sinkhorn_loop(culamp_handle h, int n, int m, int d, double p, double eta, double winf,
+                  const culamp_args *args, int64_t frequency, uint32_t flags, int64_t log_cap,
+                  cudaStream_t st, Ctl *out_ctl, float *ms) {
+    Solver &S = *h->solver;
+    Ctl c;
+    std::memset(&c, 0, sizeof(c));
+    c.itermax = args->itermax;
+    c.frequency = frequency;
+    c.stop = args->itermax < 1;
+    c.stop_reason = args->itermax < 1 ? 2 : 0;
+    c.tmax_s = args->tmax;
+    c.epsilon = args->epsilon;
+    c.eta = eta;
+    c.winf = winf;
+    c.log = S.logbuf.as<culamp_log_row>();
+    c.log_cap = log_cap;
+    CUDA_TRY(h, cudaMemcpyAsync(S.ctl.ptr, &c, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+    set_start_kernel<<<1, 1, 0, st>>>(S.ctl.as<Ctl>());
+    SkPlan pl = make_sk_plan(h, n, m, d, p, flags);
+    auto body = [&](cudaStream_t s) -> cudaError_t {
+        cudaError_t e = launch_pass(pl.k1, pl.pm_iter, ACC_LSE, pl.s_rows, S.scr, s);
+        if (e == cudaSuccess) e = launch_pass(pl.k2, pl.pm_iter, ACC_LSE, pl.s_cols, S.scr, s);
+        if (e == cudaSuccess) e = launch_pass(pl.k3, pl.pm_resid, ACC_LSE, pl.s_rows, S.scr, s);
+        return e;
+    };
+    CUDA_TRY(h, cudaEventRecord(S.ev0, st));
+    if (flags & CULAMP_FLAG_NO_GRAPH) {
+        // host-driven loop: check the stop flag after every iteration
+        for (long long it = 0; it < args->itermax + 2; ++it) {
+            CUDA_TRY(h, body(st));
+            int stop = 0;
+            CUDA_TRY(h, cudaMemcpyAsync(&stop, &S.ctl.as<Ctl>()->stop, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CUDA_TRY(h, cudaStreamSynchronize(st));
+            if (stop) break;
+        }
+    } else {
+        GraphKey key;
+        key.kind = KIND_SK;
+        key.n = n; key.m = m; key.d = d;
+        key.pm_iter = pl.pm_iter; key.pm_resid = pl.pm_resid;
+        key.p = p;
+        key.unroll = pick_unroll((double)n * m * (frequency == 1 ? 3.0 : 2.0));
+        key.generation = S.generation;
+        cudaGraphExec_t ex = nullptr;
+        int s = get_graph(h, key, body, &ex);
+        if (s) return s;
+        CUDA_TRY(h, cudaGraphLaunch(ex, st));
+    }
+    CUDA_TRY(h, cudaEventRecord(S.ev1, st));
+    CUDA_TRY(h, cudaMemcpyAsync(out_ctl, S.ctl.ptr, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    CUDA_TRY(h, cudaEventElapsedTime(ms, S.ev0, S.ev1));
+    if (out_ctl->error) return culamp_set_error(h, CULAMP_ERR_DEVICE_TIMEOUT, "loop control bound hit");
+    return CULAMP_OK;
+}
+
+// Final residual_opt! pass (SinkhornKernel.jl:541-544): residual L1 and transport cost.
+int sinkhorn_final(culamp_handle h, int n, int m, int d, double p, double eta, double winf,
+                   uint32_t flags, cudaStream_t st, double *resid, double *obj) {
+    Solver &S = *h->solver;
+    SkPlan pl = make_sk_plan(h, n, m, d, p, flags);
+    PassParams P = pl.k3;
+    P.ctl = h->pass_ctl.as<Ctl>();
+    P.gate = GATE_ALWAYS;
+    P.coef_mode = COEF_FIXED;
+    P.alpha = -1.0 / (eta * winf);
+    P.beta = 1.0;
+    P.finish = FIN_SUMS;
+    CUDA_TRY(h, launch_pass(P, pl.pm_resid, ACC_LSE, pl.s_rows, S.scr, st));
+    double sums[4];
+    CUDA_TRY(h, cudaMemcpyAsync(sums, h->pass_ctl.as<Ctl>()->sums, sizeof(sums), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    *resid = sums[0];
+    *obj = sums[1];
+    return CULAMP_OK;
+}
+
+}  // namespace
+
+extern "C" int culamp_sinkhorn(culamp_handle h, const double *x, const double *y, int64_t n,
+                               int64_t m, int32_t d, const double *r, const double *c,
+                               const culamp_args *args, int64_t frequency, double p,
+                               const double *phi0, const double *psi0, uint32_t flags,
+                               double *phi, double *psi, culamp_stats *stats, culamp_log_row *log,
+                               int64_t log_cap, void *stream) {
+    int s = check_solver_args(h, x, y, n, m, d, r, c, args, frequency, p);
+    if (s) return s;
+    if (!phi || !psi) return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "null output pointer");
+    if (!(args->eta_p > 0.0))
+        return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "Sinkhorn needs eta_p > 0 (got %g)", args->eta_p);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (flags & CULAMP_FLAG_FORM_PLAIN)
+        return culamp_plain_sinkhorn(h, x, y, n, m, d, r, c, args, frequency, p, phi0, psi0, flags,
+                                     phi, psi, stats, log, log_cap, st);
+    s = ensure_solver(h, (int)n, (int)m, d, log ? log_cap : 0);
+    if (s) return s;
+    Solver &S = *h->solver;
+    s = stage_inputs(h, x, y, (int)n, (int)m, d, r, c, st, nullptr);
+    if (s) return s;
+    if (phi0) CUDA_TRY(h, cudaMemcpyAsync(S.phi.ptr, phi0, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    else CUDA_TRY(h, cudaMemsetAsync(S.phi.ptr, 0, n * sizeof(double), st));
+    if (psi0) CUDA_TRY(h, cudaMemcpyAsync(S.psi.ptr, psi0, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    else CUDA_TRY(h, cudaMemsetAsync(S.psi.ptr, 0, m * sizeof(double), st));
+    double winf = 0.0;
+    s = compute_winf(h, (int)n, (int)m, d, p, st, &winf);
+    if (s) return s;
+    Ctl hc;
+    float ms = 0.f;
+    s = sinkhorn_loop(h, (int)n, (int)m, d, p, args->eta_p, winf, args, frequency, flags,
+                      log ? log_cap : 0, st, &hc, &ms);
+    if (s) return s;
+    double resid = 0, obj = 0;
+    s = sinkhorn_final(h, (int)n, (int)m, d, p, args->eta_p, winf, flags, st, &resid, &obj);
+    if (s) return s;
+    CUDA_TRY(h, cudaMemcpyAsync(phi, S.phi.ptr, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemcpyAsync(psi, S.psi.ptr, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    s = copy_log(h, hc, log, log_cap, st);
+    if (s) return s;
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        fill_stats_common(stats, hc, ms);
+        stats->residual = resid;
+        stats->objective = obj;
+        stats->winf = winf;
+        stats->eta_t = NAN;
+        stats->s_t = NAN;
+    }
+    return CULAMP_OK;
+}
+
+// ---------------------------------------------------------------------- LAMP
+
+namespace {
+
+struct LampPlan {
+    PassParams k1, k2, kd, k3, k4;
+    int pm;
+    bool dual_min;
+    LaunchShape s_rows, s_cols;
+};
+
+LampPlan make_lamp_plan(culamp_handle h, int n, int m, int d, double p, double winf, double eta,
+                        const culamp_args *args) {
+    Solver &S = *h->solver;
+    Ctl *ctl = S.ctl.as<Ctl>();
+    LampPlan pl;
+    pl.pm = pmode_of(p);
+    double *X = S.X.as<double>(), *Y = S.Y.as<double>();
+    const double minv = std::tanh(-args->B / 2.0), maxv = std::tanh(args->B / 2.0);
+    // K1: logZ_i = LSE_j(-(C s/(2W) + nu_j)/eta_t); phi_i = log r_i - logZ_i
+    pl.k1 = mk(X, Y, n, m, d, p, ctl);
+    pl.k1.ctr = X;
+    pl.k1.epi = EPI_LOGZ;
+    pl.k1.coef_mode = COEF_SPP_CUR;
+    pl.k1.colpot = S.nu.as<double>();
+    pl.k1.marg = S.r.as<double>();
+    pl.k1.out = S.logz.as<double>();
+    pl.k1.aux = S.aux.as<double>();
+    pl.k1.finish = FIN_LAMP_Z;
+    // K2: column residual at nu (+ cost on check iterations), fused theta_bar / nu_bar step
+    pl.k2 = mk(Y, X, m, n, d, p, ctl);
+    pl.k2.ctr = X;
+    pl.k2.epi = EPI_SPP_COL;
+    pl.k2.coef_mode = COEF_SPP_CUR;
+    pl.k2.colpot = S.aux.as<double>();
+    pl.k2.colpot_unit = 1;
+    pl.k2.rowpot = S.nu.as<double>();
+    pl.k2.cvec = S.c.as<double>();
+    pl.k2.out = S.res.as<double>();
+    pl.k2.out2 = S.cost.as<double>();
+    pl.k2.want_moment = 2;
+    pl.k2.lamp_step = LAMP_A;
+    pl.k2.theta = S.theta.as<double>();
+    pl.k2.thetab = S.thetab.as<double>();
+    pl.k2.nu = S.nu.as<double>();
+    pl.k2.nub = S.nub.as<double>();
+    pl.k2.eta_mu_i = S.eta_mu.as<double>();
+    pl.k2.eta_mu_exp = args->eta_mu;
+    pl.k2.minv = minv;
+    pl.k2.maxv = maxv;
+    pl.k2.finish = FIN_LAMP_A;
+    // Kd (check iterations): dual value at theta
+    pl.dual_min = !(eta > 0.0);
+    pl.kd = mk(X, Y, n, m, d, p, ctl);
+    pl.kd.marg = S.r.as<double>();
+    pl.kd.colpot = S.theta.as<double>();
+    pl.kd.out = S.tmp.as<double>();
+    pl.kd.gate = GATE_CHECK;
+    pl.kd.finish = FIN_LAMP_DUAL;
+    if (pl.dual_min) {
+        pl.kd.epi = EPI_RAW;
+        pl.kd.minmax_scale = 2.0 * winf;
+    } else {
+        pl.kd.ctr = X;
+        pl.kd.epi = EPI_LOGZ;
+        pl.kd.coef_mode = COEF_SPP_DUAL;
+    }
+    // K3: logZ at nu_bar with (eta_t', s')
+    pl.k3 = pl.k1;
+    pl.k3.coef_mode = COEF_SPP_NEXT;
+    pl.k3.colpot = S.nub.as<double>();
+    pl.k3.finish = FIN_NONE;
+    // K4: column residual at nu_bar, fused theta / nu step, iteration bookkeeping
+    pl.k4 = pl.k2;
+    pl.k4.coef_mode = COEF_SPP_NEXT;
+    pl.k4.rowpot = S.nub.as<double>();
+    pl.k4.want_moment = 0;
+    pl.k4.lamp_step = LAMP_B;
+    pl.k4.finish = FIN_LAMP_B;
+    pl.s_rows = pass_shape(n, m, d, ACC_LSE, h->sm_count);
+    pl.s_cols = pass_shape(m, n, d, ACC_LSE, h->sm_count);
+    return pl;
+}
+
+}  // namespace
+
+extern "C" int culamp_lamp(culamp_handle h, const double *x, const double *y, int64_t n, int64_t m,
+                           int32_t d, const double *r, const double *c, const culamp_args *args,
+                           int64_t frequency, double p, uint32_t flags, double *nu, double *phi,
+                           double *psi, double *theta, culamp_stats *stats, culamp_log_row *log,
+                           int64_t log_cap, void *stream) {
+    int s = check_solver_args(h, x, y, n, m, d, r, c, args, frequency, p);
+    if (s) return s;
+    if (!(args->eta_p >= 0.0))
+        return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "LAMP needs eta_p >= 0 (got %g)", args->eta_p);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (flags & CULAMP_FLAG_FORM_PLAIN)
+        return culamp_plain_lamp(h, x, y, n, m, d, r, c, args, frequency, p, flags, nu, phi, psi,
+                                 theta, stats, log, log_cap, st);
+    s = ensure_solver(h, (int)n, (int)m, d, log ? log_cap : 0);
+    if (s) return s;
+    Solver &S = *h->solver;
+    double sum_rlogr = 0.0;
+    s = stage_inputs(h, x, y, (int)n, (int)m, d, r, c, st, &sum_rlogr);
+    if (s) return s;
+    double winf = 0.0;
+    s = compute_winf(h, (int)n, (int)m, d, p, st, &winf);
+    if (s) return s;
+    const double eta = args->eta_p / (2.0 * winf);
+    CUDA_TRY(h, cudaMemsetAsync(S.theta.ptr, 0, m * sizeof(double), st));
+    CUDA_TRY(h, cudaMemsetAsync(S.nu.ptr, 0, m * sizeof(double), st));
+    CUDA_TRY(h, cudaMemsetAsync(S.thetab.ptr, 0, m * sizeof(double), st));
+    CUDA_TRY(h, cudaMemsetAsync(S.nub.ptr, 0, m * sizeof(double), st));
+    eta_mu_kernel<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(S.eta_mu.as<double>(), S.c.as<double>(),
+                                                               args->alpha / (double)n, args->tau_mu, m);
+    CUDA_TRY(h, cudaGetLastError());
+    Ctl hc0;
+    std::memset(&hc0, 0, sizeof(hc0));
+    hc0.itermax = args->itermax;
+    hc0.frequency = frequency;
+    hc0.stop = args->itermax < 1;
+    hc0.stop_reason = args->itermax < 1 ? 2 : 0;
+    hc0.check_enabled = args->verbose || (flags & CULAMP_FLAG_CHECK_ALWAYS);
+    hc0.do_check = hc0.check_enabled;
+    hc0.marginal_only = (flags & CULAMP_FLAG_MARGINAL_ONLY) ? 1 : 0;
+    hc0.tmax_s = args->tmax;
+    hc0.epsilon = args->epsilon;
+    hc0.winf = winf;
+    hc0.eta_lamp = eta;
+    hc0.eta_t = INFINITY;
+    hc0.s_t = 1.0;
+    hc0.tau_p = 1.0;   // hard-coded in the reference (MirrorProxKernel.jl:1073)
+    hc0.hr = eta * sum_rlogr;
+    hc0.log = S.logbuf.as<culamp_log_row>();
+    hc0.log_cap = log ? log_cap : 0;
+    CUDA_TRY(h, cudaMemcpyAsync(S.ctl.ptr, &hc0, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+    set_start_kernel<<<1, 1, 0, st>>>(S.ctl.as<Ctl>());
+    LampPlan pl = make_lamp_plan(h, (int)n, (int)m, d, p, winf, eta, args);
+    auto body = [&](cudaStream_t cs) -> cudaError_t {
+        cudaError_t e = launch_pass(pl.k1, pl.pm, ACC_LSE, pl.s_rows, S.scr, cs);
+        if (e == cudaSuccess) e = launch_pass(pl.k2, pl.pm, ACC_LSE, pl.s_cols, S.scr, cs);
+        if (e == cudaSuccess)
+            e = launch_pass(pl.kd, pl.pm, pl.dual_min ? ACC_MIN : ACC_LSE, pl.s_rows, S.scr, cs);
+        if (e == cudaSuccess) e = launch_pass(pl.k3, pl.pm, ACC_LSE, pl.s_rows, S.scr, cs);
+        if (e == cudaSuccess) e = launch_pass(pl.k4, pl.pm, ACC_LSE, pl.s_cols, S.scr, cs);
+        return e;
+    };
+    CUDA_TRY(h, cudaEventRecord(S.ev0, st));
+    if (flags & CULAMP_FLAG_NO_GRAPH) {
+        for (long long it = 0; it < args->itermax + 2; ++it) {
+            CUDA_TRY(h, body(st));
+            int stop = 0;
+            CUDA_TRY(h, cudaMemcpyAsync(&stop, &S.ctl.as<Ctl>()->stop, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CUDA_TRY(h, cudaStreamSynchronize(st));
+            if (stop) break;
+        }
+    } else {
+        GraphKey key;
+        key.kind = KIND_LAMP;
+        key.n = (int)n; key.m = (int)m; key.d = d;
+        key.pm_iter = pl.pm;
+        key.pm_resid = pl.dual_min ? 1 : 0;
+        key.unroll = pick_unroll((double)n * m * 4.0);
+        key.generation = S.generation;
+        key.p = p;
+        key.winf = winf;
+        key.B = args->B;
+        key.eta_mu = args->eta_mu;
+        cudaGraphExec_t ex = nullptr;
+        s = get_graph(h, key, body, &ex);
+        if (s) return s;
+        CUDA_TRY(h, cudaGraphLaunch(ex, st));
+    }
+    CUDA_TRY(h, cudaEventRecord(S.ev1, st));
+    Ctl hc;
+    CUDA_TRY(h, cudaMemcpyAsync(&hc, S.ctl.ptr, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    float ms = 0.f;
+    CUDA_TRY(h, cudaEventElapsedTime(&ms, S.ev0, S.ev1));
+    if (hc.error) return culamp_set_error(h, CULAMP_ERR_DEVICE_TIMEOUT, "loop control bound hit");
+    // post-loop (MirrorProxKernel.jl:1124-1129): logZ at (nu, eta_t, s), phi, psi;
+    // then the column residual / cost of the returned state.
+    {
+        Ctl *pc = h->pass_ctl.as<Ctl>();
+        PassParams a = pl.k1;
+        a.ctl = pc;
+        a.coef_mode = COEF_FIXED;
+        const double c1 = hc.s_t / (2.0 * winf), invreg = 1.0 / hc.eta_t;
+        a.alpha = -c1 * invreg;
+        a.beta = -invreg;
+        a.finish = FIN_NONE;
+        CUDA_TRY(h, launch_pass(a, pl.pm, ACC_LSE, pl.s_rows, S.scr, st));
+        PassParams b = pl.k2;
+        b.ctl = pc;
+        b.coef_mode = COEF_FIXED;
+        b.alpha = a.alpha;
+        b.beta = a.beta;
+        b.lamp_step = LAMP_NONE;
+        b.want_moment = 1;
+        b.finish = FIN_SUMS;
+        CUDA_TRY(h, launch_pass(b, pl.pm, ACC_LSE, pl.s_cols, S.scr, st));
+    }
+    double sums[4];
+    CUDA_TRY(h, cudaMemcpyAsync(sums, h->pass_ctl.as<Ctl>()->sums, sizeof(sums), cudaMemcpyDeviceToHost, st));
+    if (phi) CUDA_TRY(h, cudaMemcpyAsync(phi, S.aux.ptr, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (nu) CUDA_TRY(h, cudaMemcpyAsync(nu, S.nu.ptr, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (theta) CUDA_TRY(h, cudaMemcpyAsync(theta, S.theta.ptr, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (psi) {
+        // psi = -2 W_inf nu / eta_p (NaN / Inf when eta_p = 0, as in the reference)
+        scale_kernel<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(psi, S.nu.as<double>(),
+                                                                  -2.0 * winf / args->eta_p, m);
+        CUDA_TRY(h, cudaGetLastError());
+    }
+    s = copy_log(h, hc, log, log_cap, st);
+    if (s) return s;
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        fill_stats_common(stats, hc, ms);
+        stats->num_iter = hc.iter;
+        stats->residual = sums[0];
+        stats->objective = sums[1];
+        stats->winf = winf;
+        stats->eta_t = hc.eta_t;
+        stats->s_t = hc.s_t;
+    }
+    return CULAMP_OK;
+}
+
+// --------------------------------------------------------- annealed Sinkhorn
+
+extern "C" int culamp_annealed_sinkhorn(culamp_handle h, const double *x, const double *y,
+                                        int64_t n, int64_t m, int32_t d, const double *r,
+                                        const double *c, const culamp_args *args,
+                                        int64_t frequency, double p, uint32_t flags, double *phi,
+                                        double *psi, culamp_stats *stats, culamp_log_row *log,
+                                        int64_t log_cap, void *stream) {
+    int s = check_solver_args(h, x, y, n, m, d, r, c, args, frequency, p);
+    if (s) return s;
+    if (!phi || !psi) return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "null output pointer");
+    const double eta_final = args->epsilon;   // AnnealedSinkhorn.jl:162 (Q4)
+    if (!(eta_final > 0.0))
+        return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "annealed Sinkhorn needs epsilon > 0");
+    if (!(args->anneal_mult > 0.0 && args->anneal_mult < 1.0) && args->eta_p > eta_final)
+        return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "anneal_mult must be in (0, 1)");
+    if (flags & CULAMP_FLAG_FORM_PLAIN)
+        return culamp_set_error(h, CULAMP_ERR_UNSUPPORTED, "annealed Sinkhorn has no plain form");
+    cudaStream_t st = (cudaStream_t)stream;
+    s = ensure_solver(h, (int)n, (int)m, d, 0);
+    if (s) return s;
+    Solver &S = *h->solver;
+    s = stage_inputs(h, x, y, (int)n, (int)m, d, r, c, st, nullptr);
+    if (s) return s;
+    double winf = 0.0;
+    s = compute_winf(h, (int)n, (int)m, d, p, st, &winf);
+    if (s) return s;
+    // phi = log r, psi = log c; warm starts and previous values start there too
+    const unsigned bn = (unsigned)((n + 255) / 256), bm = (unsigned)((m + 255) / 256);
+    log_kernel<<<bn, 256, 0, st>>>(S.ws_phi.as<double>(), S.r.as<double>(), n);
+    log_kernel<<<bm, 256, 0, st>>>(S.ws_psi.as<double>(), S.c.as<double>(), m);
+    CUDA_TRY(h, cudaMemcpyAsync(S.prev_phi.ptr, S.ws_phi.ptr, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemcpyAsync(S.prev_psi.ptr, S.ws_psi.ptr, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    double eta = args->eta_p > eta_final ? args->eta_p : eta_final;
+    double preveta = 1.0;
+    const double q = args->anneal_mult;
+    culamp_args a = *args;
+    a.verbose = 0;
+    long long total_iters = 0, stages = 0;
+    float total_ms = 0.f;
+    double resid = NAN, obj = NAN;
+    int64_t rows = 0;
+    Ctl hc;
+    std::memset(&hc, 0, sizeof(hc));
+    auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        a.eta_p = eta;
+        CUDA_TRY(h, cudaMemcpyAsync(S.phi.ptr, S.ws_phi.ptr, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(h, cudaMemcpyAsync(S.psi.ptr, S.ws_psi.ptr, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        float ms = 0.f;
+        s = sinkhorn_loop(h, (int)n, (int)m, d, p, eta, winf, &a, frequency, flags, 0, st, &hc, &ms);
+        if (s) return s;
+        s = sinkhorn_final(h, (int)n, (int)m, d, p, eta, winf, flags, st, &resid, &obj);
+        if (s) return s;
+        total_ms += ms;
+        total_iters += hc.num_iter;
+        stages += 1;
+        const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        a.tmax = args->tmax - el;
+        if (log && rows < log_cap) {
+            culamp_log_row &lr = log[rows++];
+            lr.time_s = el;
+            lr.iter = (double)total_iters;
+            lr.infeas = resid;
+            lr.ot_objective = obj;
+            lr.primal = NAN;
+            lr.dual = eta;   // the reference prints eta in this column
+        }
+        if (eta == eta_final || el >= args->tmax) break;
+        const double f = eta / preveta;
+        extrapolate_kernel<<<bn, 256, 0, st>>>(S.ws_phi.as<double>(), S.prev_phi.as<double>(), S.phi.as<double>(), f, n);
+        extrapolate_kernel<<<bm, 256, 0, st>>>(S.ws_psi.as<double>(), S.prev_psi.as<double>(), S.psi.as<double>(), f, m);
+        CUDA_TRY(h, cudaGetLastError());
+        preveta = eta;
+        eta = q * eta > eta_final ? q * eta : eta_final;
+    }
+    CUDA_TRY(h, cudaMemcpyAsync(phi, S.phi.ptr, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemcpyAsync(psi, S.psi.ptr, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->iterations = stages;
+        stats->num_iter = total_iters;
+        stats->residual = resid;
+        stats->objective = obj;
+        stats->winf = winf;
+        stats->eta_t = eta;
+        stats->s_t = NAN;
+        stats->elapsed_ms = total_ms;
+        stats->log_rows = rows;
+        stats->stopped = hc.stop_reason;
+        stats->status = CULAMP_OK;
+    }
+    return CULAMP_OK;
+}
+
+// ------------------------------------------------------------- host variants
+
+namespace {
+struct HostStage {
+    culamp_handle h;
+    std::vector<std::pair<void *, size_t>> allocs;
+    ~HostStage() {
+        for (auto &a : allocs) cudaFree(a.first);
+    }
+    double *put(const double *src, size_t count, cudaStream_t st, int *err) {
+        void *p = nullptr;
+        if (cudaMalloc(&p, count * sizeof(double) + 8) != cudaSuccess) { *err = CULAMP_ERR_ALLOC; return nullptr; }
+        allocs.push_back({p, count});
+        if (src && cudaMemcpyAsync(p, src, count * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess)
+            *err = CULAMP_ERR_CUDA;
+        return (double *)p;
+    }
+};
+}  // namespace
+
+extern "C" int culamp_sinkhorn_host(culamp_handle h, const double *x, const double *y, int64_t n,
+                                    int64_t m, int32_t d, const double *r, const double *c,
+                                    const culamp_args *args, int64_t frequency, double p,
+                                    const double *phi0, const double *psi0, uint32_t flags,
+                                    double *phi, double *psi, culamp_stats *stats,
+                                    culamp_log_row *log, int64_t log_cap) {
+    int s = check_solver_args(h, x, y, n, m, d, r, c, args, frequency, p);
+    if (s) return s;
+    if (!phi || !psi) return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "null output pointer");
+    cudaStream_t st = nullptr;
+    HostStage hs{h, {}};
+    int err = 0;
+    double *dx = hs.put(x, (size_t)n * d, st, &err), *dy = hs.put(y, (size_t)m * d, st, &err);
+    double *dr = hs.put(r, n, st, &err), *dc = hs.put(c, m, st, &err);
+    double *dphi0 = phi0 ? hs.put(phi0, n, st, &err) : nullptr;
+    double *dpsi0 = psi0 ? hs.put(psi0, m, st, &err) : nullptr;
+    double *dphi = hs.put(nullptr, n, st, &err), *dpsi = hs.put(nullptr, m, st, &err);
+    if (err) return culamp_set_error(h, err, "host staging failed");
+    s = culamp_sinkhorn(h, dx, dy, n, m, d, dr, dc, args, frequency, p, dphi0, dpsi0, flags, dphi,
+                        dpsi, stats, log, log_cap, st);
+    if (s) return s;
+    CUDA_TRY(h, cudaMemcpyAsync(phi, dphi, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaMemcpyAsync(psi, dpsi, m * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    return CULAMP_OK;
+}
+
+extern "C" int culamp_lamp_host(culamp_handle h, const double *x, const double *y, int64_t n,
+                                int64_t m, int32_t d, const double *r, const double *c,
+                                const culamp_args *args, int64_t frequency, double p,
+                                uint32_t flags, double *nu, double *phi, double *psi,
+                                double *theta, culamp_stats *stats, culamp_log_row *log,
+                                int64_t log_cap) {
+    int s = check_solver_args(h, x, y, n, m, d, r, c, args, frequency, p);
+    if (s) return s;
+    cudaStream_t st = nullptr;
+    HostStage hs{h, {}};
+    int err = 0;
+    double *dx = hs.put(x, (size_t)n * d, st, &err), *dy = hs.put(y, (size_t)m * d, st, &err);
+    double *dr = hs.put(r, n, st, &err), *dc = hs.put(c, m, st, &err);
+    double *dnu = hs.put(nullptr, m, st, &err), *dphi = hs.put(nullptr, n, st, &err);
+    double *dpsi = hs.put(nullptr, m, st, &err), *dth = hs.put(nullptr, m, st, &err);
+    if (err) return culamp_set_error(h, err, "host staging failed");
+    s = culamp_lamp(h, dx, dy, n, m, d, dr, dc, args, frequency, p, flags, dnu, dphi, dpsi, dth,
+                    stats, log, log_cap, st);
+    if (s) return s;
+    if (nu) CUDA_TRY(h, cudaMemcpyAsync(nu, dnu, m * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (phi) CUDA_TRY(h, cudaMemcpyAsync(phi, dphi, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (psi) CUDA_TRY(h, cudaMemcpyAsync(psi, dpsi, m * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (theta) CUDA_TRY(h, cudaMemcpyAsync(theta, dth, m * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    return CULAMP_OK;
+}

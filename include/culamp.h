@@ -1,0 +1,213 @@
+/*
+ * culamp.h -- C ABI of libculamp_b200, a B200-native (sm_100a) implementation of
+ * CuLAMP.jl's kernelized entropic optimal-transport path: the fused on-the-fly
+ * cost plus online log-sum-exp row / column reductions behind the `lamp`,
+ * `sinkhorn` and `annealed_sinkhorn` `--kernel` solvers.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (CULAMP_OK = 0) and never throws.
+ *    culamp_last_error() gives a one-line reason for the last failure on a handle.
+ *  - Arrays are FP64, as in every shipped reference run (CmdLineUtils.jl:208 builds
+ *    Float64 coordinates). Coordinates are point-major: x[i*d + k]. The reference's
+ *    3 x N column-major CuArray (img[k, i]) has exactly this memory layout, so a
+ *    Julia caller passes pointer(img) unchanged.
+ *  - "Device" entry points take device pointers in caller-owned memory and a CUDA
+ *    stream (cudaStream_t passed as void*, NULL = legacy default stream); they are
+ *    asynchronous unless stated. "_host" entry points take host pointers, copy in,
+ *    solve and copy out synchronously.
+ *  - Cost C(x, y) is the reference's: p = 1 -> sum|d|, p = 2 -> sum d^2 (squared,
+ *    no root), p = Inf -> max|d|, any other p > 0 -> sum |d|^p (no root).
+ *  - A handle owns its workspace and CUDA graphs; use one handle per host thread.
+ */
+#ifndef CULAMP_H
+#define CULAMP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CULAMP_VERSION 100
+
+/* status codes */
+#define CULAMP_OK                 0
+#define CULAMP_ERR_INVALID_ARG    1   /* bad size, pointer, p, eta, marginal ...     */
+#define CULAMP_ERR_CUDA           2   /* a CUDA runtime call failed                  */
+#define CULAMP_ERR_ALLOC          3   /* device or host allocation failed            */
+#define CULAMP_ERR_UNSUPPORTED    4   /* valid but not implemented (e.g. d > 16)     */
+#define CULAMP_ERR_IO             5   /* settings / potential file could not be read */
+#define CULAMP_ERR_DEVICE_TIMEOUT 6   /* a bounded device-side wait gave up          */
+
+/* Solver option bits. 0 reproduces the reference's behaviour. */
+#define CULAMP_FLAG_TRUE_PINF      1u  /* Sinkhorn p=Inf iterates on the true L-inf cost.
+                                          Default follows SinkhornKernel.jl:518-520, whose
+                                          _opt kernel evaluates squared-Euclidean for p=Inf. */
+#define CULAMP_FLAG_CHECK_ALWAYS   2u  /* LAMP: run the convergence check every `frequency`
+                                          iterations even when args.verbose == 0
+                                          (MirrorProxKernel.jl:1081 checks only when verbose) */
+#define CULAMP_FLAG_MARGINAL_ONLY  4u  /* LAMP: stop on the marginal test alone           */
+#define CULAMP_FLAG_FORM_PLAIN     8u  /* plain FP32 form: the reference's kernel shape
+                                          (warp per row, FP32 potentials, host-synchronised
+                                          loop). Default is the chosen form.               */
+#define CULAMP_FLAG_NO_GRAPH      16u  /* chosen form without CUDA graphs (debugging)      */
+
+/* EOTArgs (src/Utilities.jl:18-31), same field names and defaults. */
+typedef struct culamp_args {
+    double eta_p, eta_mu, tau_p, tau_mu, alpha, B, epsilon, anneal_mult;
+    int64_t itermax, inner_iter;
+    double tmax;
+    int32_t verbose;
+    int32_t _pad;
+} culamp_args;
+
+/* One row of the convergence log the reference prints:
+ * time(s),iter,infeas,ot_objective,primal,dual (SinkhornKernel.jl:533,
+ * MirrorProxKernel.jl:1097). Fields a solver does not print are NaN
+ * (annealed Sinkhorn stores eta in `dual`). */
+typedef struct culamp_log_row {
+    double time_s, iter, infeas, ot_objective, primal, dual;
+} culamp_log_row;
+
+typedef struct culamp_stats {
+    int64_t iterations;   /* loop index reached (iterations whose updates ran)        */
+    int64_t num_iter;     /* the reference's num_iter counter (SinkhornKernel.jl:539) */
+    double residual;      /* final L1 marginal residual                               */
+    double objective;     /* final transport cost sum(P .* C) (sum of the cost cache) */
+    double winf;          /* max-cost normaliser W_inf                                 */
+    double eta_t, s_t;    /* LAMP: final eta_t and s                                   */
+    double elapsed_ms;    /* device time of the solve                                  */
+    int64_t log_rows;     /* rows written to the caller's log buffer                   */
+    int32_t stopped;      /* 1 = tolerance met, 2 = itermax, 3 = tmax                  */
+    int32_t status;
+} culamp_stats;
+
+typedef struct culamp_handle_s *culamp_handle;
+
+/* ---------------------------------------------------------------- handle */
+int culamp_version(void);
+int culamp_create(culamp_handle *out, int device);
+int culamp_destroy(culamp_handle h);
+const char *culamp_status_string(int status);
+const char *culamp_last_error(culamp_handle h);
+
+/* ---------------------------------------------------------------- settings */
+/* Defaults of EOTArgs (Utilities.jl:18-31). */
+int culamp_args_default(culamp_args *out);
+/* read_args_json (Utilities.jl:88-92): JSON object with any subset of the EOTArgs
+ * keys; missing keys keep their defaults, unknown keys are ignored. */
+int culamp_args_from_json(const char *path, culamp_args *out);
+int culamp_args_from_json_string(const char *json, culamp_args *out);
+
+/* ------------------------------------------------------ pass-level kernels
+ * Device pointers, asynchronous on `stream`. Scratch comes from the handle. */
+
+/* max_logsumexp_spp_ct! (MirrorProxKernel.jl:280-326): rowmax[i] = max_j C(x_i, y_j)
+ * (rowmax may be NULL); *winf_host (may be NULL) receives max_i rowmax[i]
+ * (SinkhornKernel.jl:500-502) -- this one call synchronises the stream. */
+int culamp_max_cost(culamp_handle h, const double *x, const double *y, int64_t n, int64_t m,
+                    int32_t d, double p, double *rowmax, double *winf_host, void *stream);
+
+/* warp_logsumexp_ct_fused! (SinkhornKernel.jl:341-444):
+ * out[i] = log(marg[i]) - LSE_j(-C(x_i,y_j)/(reg*winf) + pot[j]). */
+int culamp_lse_rows_sk(culamp_handle h, double *out, const double *x, const double *y,
+                       int64_t n, int64_t m, int32_t d, const double *marg, const double *pot,
+                       double reg, double winf, double p, void *stream);
+
+/* residual_opt! (SinkhornKernel.jl:9-81): res[i] = marg[i] - sum_j P_ij,
+ * cost[i] = sum_j P_ij C_ij with P_ij = exp(-C_ij/(reg*winf) + phi[i] + psi[j]).
+ * The reference evaluates C here as p==1 ? L1 : squared (SinkhornKernel.jl:38-42);
+ * pass that p to reproduce it. */
+int culamp_residual_sk(culamp_handle h, double *res, double *cost, const double *x,
+                       const double *y, int64_t n, int64_t m, int32_t d, const double *marg,
+                       const double *phi, const double *psi, double reg, double winf, double p,
+                       void *stream);
+
+/* warp_logsumexp_spp_ct_fused! (MirrorProxKernel.jl:833-938):
+ * out[i] = LSE_j(-(C_ij * st/(2 winf) + theta[j]) / reg). reg = +Inf is allowed. */
+int culamp_lse_rows_spp(culamp_handle h, double *out, const double *x, const double *y,
+                        int64_t n, int64_t m, int32_t d, const double *theta, double reg,
+                        double st, double winf, double p, void *stream);
+
+/* residual_spp_c! (MirrorProxKernel.jl:7-94), one output per column j:
+ * res[j] = sum_i marg1[i] exp(-(C_ij st/(2 winf) + theta[j])/reg - logz[i]),
+ * cost[j] = sum_i marg1[i] exp(...) C_ij. */
+int culamp_col_residual_spp(culamp_handle h, double *res, double *cost, const double *x,
+                            const double *y, int64_t n, int64_t m, int32_t d,
+                            const double *marg1, const double *theta, const double *logz,
+                            double reg, double st, double winf, double p, void *stream);
+
+/* warp_min_reduce! (MirrorProxKernel.jl:941-1016): out[i] = min_j (C_ij + 2 winf theta[j]). */
+int culamp_min_reduce(culamp_handle h, double *out, const double *x, const double *y,
+                      int64_t n, int64_t m, int32_t d, const double *theta, double winf,
+                      double p, void *stream);
+
+/* update_theta_residual (MirrorProx.jl:159-180), elementwise over m entries;
+ * theta may alias theta0. */
+int culamp_theta_update(culamp_handle h, double *theta, const double *theta0,
+                        const double *residual, const double *c, const double *eta_mu_i,
+                        double eta_mu, int32_t adjust, double minv, double maxv, double winf,
+                        int64_t m, void *stream);
+
+/* naive_findmaxindex_ct! (SinkhornKernel.jl:124-162): barycentric image
+ * out[i*d+k] = sum_j y[j*d+k] P_ij / sum_j P_ij, P_ij = exp(-C_ij/(reg winf) + phi[i] + psi[j]). */
+int culamp_barycentric_sk(culamp_handle h, double *out, const double *x, const double *y,
+                          int64_t n, int64_t m, int32_t d, const double *phi, const double *psi,
+                          double reg, double winf, double p, void *stream);
+
+/* --------------------------------------------------------- solver level
+ * Device pointers; the call returns when the solve has finished (it reads the
+ * convergence state back once per batch of graph-launched iterations).
+ * `log` (host memory, may be NULL) receives up to log_cap rows. */
+
+/* sinkhorn_color_transfer with return_assignments=false (SinkhornKernel.jl:477-559):
+ * phi (n), psi (m) in the reference's units (P_ij = exp(phi_i + psi_j - C_ij/(eta_p W_inf))).
+ * phi0 / psi0 (device, may be NULL) are warm starts. */
+int culamp_sinkhorn(culamp_handle h, const double *x, const double *y, int64_t n, int64_t m,
+                    int32_t d, const double *r, const double *c, const culamp_args *args,
+                    int64_t frequency, double p, const double *phi0, const double *psi0,
+                    uint32_t flags, double *phi, double *psi, culamp_stats *stats,
+                    culamp_log_row *log, int64_t log_cap, void *stream);
+
+/* extragradient_color_transfer without the barycentric maps (MirrorProxKernel.jl:1019-1132):
+ * nu, psi, theta (m), phi (n); psi = -2 W_inf nu / eta_p, phi = log r - logZ(nu). */
+int culamp_lamp(culamp_handle h, const double *x, const double *y, int64_t n, int64_t m,
+                int32_t d, const double *r, const double *c, const culamp_args *args,
+                int64_t frequency, double p, uint32_t flags, double *nu, double *phi,
+                double *psi, double *theta, culamp_stats *stats, culamp_log_row *log,
+                int64_t log_cap, void *stream);
+
+/* annealed_sinkhorn_euclidean, potentials only (AnnealedSinkhorn.jl:149-261):
+ * eta_p -> max(anneal_mult * eta, epsilon) stages with extrapolated warm starts;
+ * epsilon is both the final eta and the inner tolerance, as in the reference. */
+int culamp_annealed_sinkhorn(culamp_handle h, const double *x, const double *y, int64_t n,
+                             int64_t m, int32_t d, const double *r, const double *c,
+                             const culamp_args *args, int64_t frequency, double p,
+                             uint32_t flags, double *phi, double *psi, culamp_stats *stats,
+                             culamp_log_row *log, int64_t log_cap, void *stream);
+
+/* Host-buffer variants: same arguments with host pointers; copies in, solves and
+ * copies out (the end-to-end path a Julia Array caller uses). */
+int culamp_sinkhorn_host(culamp_handle h, const double *x, const double *y, int64_t n,
+                         int64_t m, int32_t d, const double *r, const double *c,
+                         const culamp_args *args, int64_t frequency, double p,
+                         const double *phi0, const double *psi0, uint32_t flags, double *phi,
+                         double *psi, culamp_stats *stats, culamp_log_row *log,
+                         int64_t log_cap);
+int culamp_lamp_host(culamp_handle h, const double *x, const double *y, int64_t n, int64_t m,
+                     int32_t d, const double *r, const double *c, const culamp_args *args,
+                     int64_t frequency, double p, uint32_t flags, double *nu, double *phi,
+                     double *psi, double *theta, culamp_stats *stats, culamp_log_row *log,
+                     int64_t log_cap);
+
+/* FP64 re-evaluation of a Sinkhorn-form plan's L1 marginal errors, exp in FP64
+ * (used to certify "1e-6 L1, FP64-checked"). Device pointers; synchronous. */
+int culamp_marginal_error_fp64(culamp_handle h, const double *x, const double *y, int64_t n,
+                               int64_t m, int32_t d, const double *r, const double *c,
+                               const double *phi, const double *psi, double reg, double winf,
+                               double p, double *row_l1, double *col_l1, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CULAMP_H */

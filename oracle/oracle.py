@@ -1,0 +1,374 @@
+"""Oracle for the kernelized entropic-OT path: TEST INFRASTRUCTURE ONLY.
+
+Two independent FP64 restatements of CuLAMP.jl's algorithms:
+
+* ``C``   -- ctypes bindings to oracle/culamp_oracle.c (OpenMP, any size the CPU
+  finishes), built by oracle/Makefile into oracle/_build/.
+* ``np_*`` -- a vectorised numpy restatement for small sizes, written separately
+  so the two can check each other.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
+arm may import this module. Parity status: partially pinned -- the reference
+cannot run here; its archived W_inf values (126 / 7938 / 63 for p = 1 / 2 / Inf
+on its integer 64x64 grid, data_archive/data/updated_pnorm.csv) are the only
+values taken from reference outputs.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libculamp_oracle.so")
+
+TRUE_PINF = 1
+CHECK_ALWAYS = 2
+MARGINAL_ONLY = 4
+
+
+class OrArgs(C.Structure):
+    _fields_ = [("eta_p", C.c_double), ("eta_mu", C.c_double), ("tau_p", C.c_double),
+                ("tau_mu", C.c_double), ("alpha", C.c_double), ("B", C.c_double),
+                ("epsilon", C.c_double), ("anneal_mult", C.c_double),
+                ("itermax", C.c_int64), ("inner_iter", C.c_int64), ("tmax", C.c_double),
+                ("verbose", C.c_int32), ("_pad", C.c_int32)]
+
+
+class OrLogRow(C.Structure):
+    _fields_ = [("time_s", C.c_double), ("iter", C.c_double), ("infeas", C.c_double),
+                ("ot_objective", C.c_double), ("primal", C.c_double), ("dual", C.c_double)]
+
+
+class OrStats(C.Structure):
+    _fields_ = [("iterations", C.c_int64), ("num_iter", C.c_int64), ("residual", C.c_double),
+                ("objective", C.c_double), ("winf", C.c_double), ("eta_t", C.c_double),
+                ("s_t", C.c_double), ("log_rows", C.c_int64), ("stopped", C.c_int32),
+                ("_pad", C.c_int32)]
+
+
+def build() -> str:
+    """Compile the C oracle (make) if missing; returns the library path."""
+    if not os.path.exists(LIB_PATH) or (
+            os.path.getmtime(LIB_PATH) < os.path.getmtime(os.path.join(HERE, "culamp_oracle.c"))):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(LIB_PATH)
+        P = C.POINTER(C.c_double)
+        i64 = C.c_int64
+        _lib.or_max_cost.restype = C.c_double
+        _lib.or_max_cost.argtypes = [P, P, i64, i64, C.c_int, C.c_double]
+        _lib.or_cost.restype = C.c_double
+        for name in ("or_sinkhorn_kernel", "or_lamp_kernel", "or_annealed_sinkhorn_kernel",
+                     "or_sinkhorn_dense", "or_lamp_dense"):
+            getattr(_lib, name).restype = C.c_int
+    return _lib
+
+
+def _p(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _c64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+@dataclass
+class Args:
+    """EOTArgs with the reference defaults (src/Utilities.jl:18-31)."""
+    eta_p: float = 0.0
+    eta_mu: float = 0.0
+    tau_p: float = 1.0
+    tau_mu: float = 1.0
+    alpha: float = 0.01
+    B: float = 1.0
+    epsilon: float = 1e-4
+    anneal_mult: float = 0.95
+    itermax: int = 10_000
+    inner_iter: int = 10
+    tmax: float = math.inf
+    verbose: bool = True
+
+    def c(self) -> OrArgs:
+        return OrArgs(self.eta_p, self.eta_mu, self.tau_p, self.tau_mu, self.alpha, self.B,
+                      self.epsilon, self.anneal_mult, int(self.itermax), int(self.inner_iter),
+                      self.tmax, int(bool(self.verbose)), 0)
+
+
+def set_threads(t: int) -> None:
+    lib().or_set_num_threads(C.c_int(t))
+
+
+def num_threads() -> int:
+    return int(lib().or_num_threads())
+
+
+def _logs(buf, st):
+    rows = []
+    for k in range(st.log_rows):
+        r = buf[k]
+        rows.append((r.time_s, int(r.iter), r.infeas, r.ot_objective, r.primal, r.dual))
+    return rows
+
+
+# ---------------------------------------------------------------- C bindings
+
+def max_cost(x, y, p):
+    x, y = _c64(x), _c64(y)
+    return lib().or_max_cost(_p(x), _p(y), x.shape[0], y.shape[0], x.shape[1], float(p))
+
+
+def max_cost_rows(x, y, p):
+    x, y = _c64(x), _c64(y)
+    out = np.empty(x.shape[0])
+    lib().or_max_cost_rows(_p(x), _p(y), C.c_int64(x.shape[0]), C.c_int64(y.shape[0]),
+                           C.c_int(x.shape[1]), C.c_double(p), _p(out))
+    return out
+
+
+def sk_lse(x, y, marg, pot, reg, winf, cost_p):
+    x, y, marg, pot = map(_c64, (x, y, marg, pot))
+    out = np.empty(x.shape[0])
+    lib().or_sk_lse(_p(out), _p(x), _p(y), C.c_int64(x.shape[0]), C.c_int64(y.shape[0]),
+                    C.c_int(x.shape[1]), _p(marg), _p(pot), C.c_double(reg), C.c_double(winf),
+                    C.c_double(cost_p))
+    return out
+
+
+def sk_residual(x, y, marg, phi, psi, reg, winf, cost_p):
+    x, y, marg, phi, psi = map(_c64, (x, y, marg, phi, psi))
+    res = np.empty(x.shape[0])
+    cost = np.empty(x.shape[0])
+    lib().or_sk_residual(_p(res), _p(cost), _p(x), _p(y), C.c_int64(x.shape[0]),
+                         C.c_int64(y.shape[0]), C.c_int(x.shape[1]), _p(marg), _p(phi),
+                         _p(psi), C.c_double(reg), C.c_double(winf), C.c_double(cost_p))
+    return res, cost
+
+
+def spp_lse(x, y, theta, reg, st, winf, p):
+    x, y, theta = map(_c64, (x, y, theta))
+    out = np.empty(x.shape[0])
+    lib().or_spp_lse(_p(out), _p(x), _p(y), C.c_int64(x.shape[0]), C.c_int64(y.shape[0]),
+                     C.c_int(x.shape[1]), _p(theta), C.c_double(reg), C.c_double(st),
+                     C.c_double(winf), C.c_double(p))
+    return out
+
+
+def spp_col_residual(x, y, marg1, theta, logz, reg, st, winf, p):
+    x, y, marg1, theta, logz = map(_c64, (x, y, marg1, theta, logz))
+    res = np.empty(y.shape[0])
+    cost = np.empty(y.shape[0])
+    lib().or_spp_col_residual(_p(res), _p(cost), _p(x), _p(y), C.c_int64(x.shape[0]),
+                              C.c_int64(y.shape[0]), C.c_int(x.shape[1]), _p(marg1), _p(theta),
+                              _p(logz), C.c_double(reg), C.c_double(st), C.c_double(winf),
+                              C.c_double(p))
+    return res, cost
+
+
+def min_reduce(x, y, theta, winf, p):
+    x, y, theta = map(_c64, (x, y, theta))
+    out = np.empty(x.shape[0])
+    lib().or_min_reduce(_p(out), _p(x), _p(y), C.c_int64(x.shape[0]), C.c_int64(y.shape[0]),
+                        C.c_int(x.shape[1]), _p(theta), C.c_double(winf), C.c_double(p))
+    return out
+
+
+def theta_update(theta0, residual, c, eta_mu_i, eta_mu, adjust, minv, maxv, winf=1.0):
+    theta0, residual, c, eta_mu_i = map(_c64, (theta0, residual, c, eta_mu_i))
+    out = np.empty_like(theta0)
+    lib().or_theta_update(_p(out), _p(theta0), _p(residual), _p(c), _p(eta_mu_i),
+                          C.c_double(eta_mu), C.c_int(int(adjust)), C.c_double(minv),
+                          C.c_double(maxv), C.c_double(winf), C.c_int64(theta0.shape[0]))
+    return out
+
+
+def barycentric_sk(x, y, phi, psi, reg, winf, cost_p):
+    x, y, phi, psi = map(_c64, (x, y, phi, psi))
+    out = np.empty_like(x)
+    lib().or_barycentric_sk(_p(out), _p(x), _p(y), C.c_int64(x.shape[0]),
+                            C.c_int64(y.shape[0]), C.c_int(x.shape[1]), _p(phi), _p(psi),
+                            C.c_double(reg), C.c_double(winf), C.c_double(cost_p))
+    return out
+
+
+def sinkhorn_kernel(x, y, r, c, args: Args, frequency=100, p=2.0, phi0=None, psi0=None,
+                    flags=0, log_cap=100000):
+    x, y, r, c = map(_c64, (x, y, r, c))
+    n, m = x.shape[0], y.shape[0]
+    phi = np.empty(n)
+    psi = np.empty(m)
+    st = OrStats()
+    buf = (OrLogRow * log_cap)()
+    a = args.c()
+    lib().or_sinkhorn_kernel(_p(x), _p(y), C.c_int64(n), C.c_int64(m), C.c_int(x.shape[1]),
+                             _p(r), _p(c), C.byref(a), C.c_int64(frequency), C.c_double(p),
+                             _p(_c64(phi0)) if phi0 is not None else None,
+                             _p(_c64(psi0)) if psi0 is not None else None,
+                             C.c_int(flags), _p(phi), _p(psi), C.byref(st), buf,
+                             C.c_int64(log_cap))
+    return phi, psi, st, _logs(buf, st)
+
+
+def lamp_kernel(x, y, r, c, args: Args, frequency=100, p=2.0, flags=0, log_cap=100000):
+    x, y, r, c = map(_c64, (x, y, r, c))
+    n, m = x.shape[0], y.shape[0]
+    nu, phi, psi, theta = np.empty(m), np.empty(n), np.empty(m), np.empty(m)
+    st = OrStats()
+    buf = (OrLogRow * log_cap)()
+    a = args.c()
+    lib().or_lamp_kernel(_p(x), _p(y), C.c_int64(n), C.c_int64(m), C.c_int(x.shape[1]),
+                         _p(r), _p(c), C.byref(a), C.c_int64(frequency), C.c_double(p),
+                         C.c_int(flags), _p(nu), _p(phi), _p(psi), _p(theta), C.byref(st), buf,
+                         C.c_int64(log_cap))
+    return nu, phi, psi, theta, st, _logs(buf, st)
+
+
+def annealed_sinkhorn_kernel(x, y, r, c, args: Args, frequency=10, p=2.0, flags=0,
+                             log_cap=10000):
+    x, y, r, c = map(_c64, (x, y, r, c))
+    n, m = x.shape[0], y.shape[0]
+    phi, psi = np.empty(n), np.empty(m)
+    st = OrStats()
+    buf = (OrLogRow * log_cap)()
+    a = args.c()
+    lib().or_annealed_sinkhorn_kernel(_p(x), _p(y), C.c_int64(n), C.c_int64(m),
+                                      C.c_int(x.shape[1]), _p(r), _p(c), C.byref(a),
+                                      C.c_int64(frequency), C.c_double(p), C.c_int(flags),
+                                      _p(phi), _p(psi), C.byref(st), buf, C.c_int64(log_cap))
+    return phi, psi, st, _logs(buf, st)
+
+
+def sinkhorn_dense(W, r, c, args: Args, frequency=50, log_cap=100000):
+    W, r, c = map(_c64, (W, r, c))
+    n = r.shape[0]
+    phi, psi = np.empty(n), np.empty(n)
+    st = OrStats()
+    buf = (OrLogRow * log_cap)()
+    a = args.c()
+    lib().or_sinkhorn_dense(_p(W), C.c_int64(n), _p(r), _p(c), C.byref(a),
+                            C.c_int64(frequency), _p(phi), _p(psi), C.byref(st), buf,
+                            C.c_int64(log_cap))
+    return phi, psi, st, _logs(buf, st)
+
+
+def lamp_dense(W, r, c, args: Args, frequency=50, log_cap=100000, want_plan=False):
+    W, r, c = map(_c64, (W, r, c))
+    n = r.shape[0]
+    theta, nu = np.empty(n), np.empty(n)
+    plan = np.empty((n, n)) if want_plan else None
+    st = OrStats()
+    buf = (OrLogRow * log_cap)()
+    a = args.c()
+    lib().or_lamp_dense(_p(W), C.c_int64(n), _p(r), _p(c), C.byref(a), C.c_int64(frequency),
+                        _p(theta), _p(nu), _p(plan), C.byref(st), buf, C.c_int64(log_cap))
+    return theta, nu, plan, st, _logs(buf, st)
+
+
+# ------------------------------------------------- independent numpy mirror
+
+def np_cost(x, y, p):
+    """Dense pair cost (small sizes). Same convention as the reference's
+    kernels: p=2 squared, p=Inf Chebyshev, other p sum |d|^p (no root)."""
+    diff = np.abs(np.asarray(x, np.float64)[:, None, :] - np.asarray(y, np.float64)[None, :, :])
+    if p == 1:
+        return diff.sum(-1)
+    if p == 2:
+        return (diff ** 2).sum(-1)
+    if math.isinf(p):
+        return diff.max(-1)
+    return (diff ** p).sum(-1)
+
+
+def np_lse(a, axis):
+    mx = a.max(axis=axis, keepdims=True)
+    return (np.log(np.exp(a - mx).sum(axis=axis, keepdims=True)) + mx).squeeze(axis)
+
+
+def np_sinkhorn_kernel(x, y, r, c, eta_p, itermax, frequency=1, epsilon=0.0, p=2.0,
+                       true_pinf=False, phi0=None, psi0=None):
+    """Sinkhorn of SinkhornKernel.jl:477-559 restated with dense numpy arrays."""
+    winf = np_cost(x, y, p).max()
+    ip = 2.0 if (math.isinf(p) and not true_pinf) else p
+    rp = p if true_pinf else (1.0 if p == 1 else 2.0)
+    Ci = np_cost(x, y, ip)
+    Cr = np_cost(x, y, rp)
+    phi = np.zeros(len(r)) if phi0 is None else np.array(phi0, np.float64)
+    psi = np.zeros(len(c)) if psi0 is None else np.array(psi0, np.float64)
+    k = -1.0 / (eta_p * winf)
+    it_done = 0
+    for it in range(1, itermax + 1):
+        phi = np.log(r) - np_lse(Ci * k + psi[None, :], 1)
+        psi = np.log(c) - np_lse(Ci.T * k + phi[None, :], 1)
+        it_done = it
+        if (it - 1) % frequency == 0:
+            P = np.exp(Cr * k + phi[:, None] + psi[None, :])
+            if np.abs(r - P.sum(1)).sum() <= epsilon / 6:
+                break
+    P = np.exp(Cr * k + phi[:, None] + psi[None, :])
+    return phi, psi, np.abs(r - P.sum(1)).sum(), (P * Cr).sum(), it_done, winf
+
+
+def np_theta_update(theta0, res, c, eta_mu_i, eta_mu, adjust, minv, maxv):
+    t = np.tanh((res - c) / eta_mu_i + 0.5 * (1 - eta_mu) * np.log((1 + theta0) / (1 - theta0)))
+    return np.clip(t, minv, maxv) if adjust else t
+
+
+def np_lamp_kernel(x, y, r, c, eta_p, itermax, p=2.0, alpha=0.01, tau_mu=1.0, eta_mu=0.0,
+                   B=1.0):
+    """LAMP of MirrorProxKernel.jl:1019-1132 (non-verbose: runs itermax)."""
+    C_ = np_cost(x, y, p)
+    winf = C_.max()
+    n, m = C_.shape
+    eta = eta_p / (2 * winf)
+    emu = (c + alpha / n) / tau_mu
+    theta = np.zeros(m)
+    nu = np.zeros(m)
+    s_t, eta_t = 1.0, math.inf
+    minv, maxv = math.tanh(-B / 2), math.tanh(B / 2)
+
+    def infeas(th, et, s):
+        if math.isinf(et):
+            A = np.zeros_like(C_)
+        else:
+            A = -(C_ * (s / (2 * winf)) + th[None, :]) / et
+        logz = np_lse(A, 1)
+        P = np.exp(A - logz[:, None]) * r[:, None]
+        return logz, P.sum(0), (P * C_).sum(0)
+
+    for _ in range(itermax):
+        _, res, _ = infeas(nu, eta_t, s_t)
+        thb = np_theta_update(theta, res, c, emu, eta_mu, False, minv, maxv)
+        eta_t = 1.0 / (1.0 + (1.0 / eta_t) * (1.0 - eta))
+        nub = (1 - eta_t) * nu + eta_t * theta
+        s_t = (1 - eta_t) * s_t + eta_t
+        _, res, _ = infeas(nub, eta_t, s_t)
+        theta = np_theta_update(theta, res, c, emu, eta_mu, True, minv, maxv)
+        nu = (1 - eta_t) * nu + eta_t * thb
+    logz, res, cost = infeas(nu, eta_t, s_t)
+    phi = np.log(r) - logz
+    psi = -2 * winf * nu / eta_p if eta_p != 0 else np.full(m, np.nan)
+    return nu, phi, psi, theta, np.abs(res - c).sum(), cost.sum(), eta_t
+
+
+def fp64_marginal_error_sk(x, y, r, c, phi, psi, eta_p, winf, p):
+    """FP64 re-evaluation of the L1 marginal errors of a Sinkhorn-form plan
+    P_ij = exp(phi_i + psi_j - C_ij/(eta_p W_inf)) via the C oracle:
+    returns (row L1, column L1)."""
+    res_r, _ = sk_residual(x, y, r, phi, psi, eta_p, winf, p)
+    res_c, _ = sk_residual(y, x, c, psi, phi, eta_p, winf, p)
+    return float(np.abs(res_r).sum()), float(np.abs(res_c).sum())
