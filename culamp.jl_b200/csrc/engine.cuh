@@ -117,6 +117,7 @@ struct Ctl {
     culamp_log_row *log;
     double sums[4];             // FIN_SUMS output
     int error;                  // device-side error code (bounded waits etc.)
+    long long loops;            // WHILE-body executions (independent loop bound)
 };
 
 struct PassParams {

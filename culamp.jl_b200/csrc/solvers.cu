@@ -43,10 +43,17 @@ namespace culamp_dev {
 
 __global__ void set_start_kernel(Ctl *c) { c->t_start_ns = globaltimer_ns(); }
 
-// Loop control of the WHILE node. The hard bound on iter makes the loop finite
-// even if a finish step never ran (it cannot exceed itermax + 2 iterations).
+// Loop control of the WHILE node. Besides the finish steps' own itermax / tmax
+// handling, the loop is bounded here independently: by the number of body
+// executions (each body runs >= 1 iteration) and by tmax, so it always ends.
 __global__ void loop_ctl_kernel(Ctl *c, cudaGraphConditionalHandle hnd) {
-    if (!c->stop && c->iter > c->itermax + 1) { c->stop = 1; c->stop_reason = 2; c->error = 1; }
+    c->loops += 1;
+    if (!c->stop && (c->iter > c->itermax + 1 || c->loops > c->itermax + 2)) {
+        c->stop = 1; c->stop_reason = 2; c->error = 1;
+    }
+    if (!c->stop && (double)(globaltimer_ns() - c->t_start_ns) * 1e-9 > c->tmax_s) {
+        c->stop = 1; c->stop_reason = 3;
+    }
     cudaGraphSetConditional(hnd, c->stop ? 0u : 1u);
 }
 
