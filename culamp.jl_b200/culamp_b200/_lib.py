@@ -96,6 +96,7 @@ SIGNATURES = {
     "culamp_lamp_host": (C.c_int, [_VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, C.POINTER(CArgs), _I64,
                                    _D, _U32, _VP, _VP, _VP, _VP, C.POINTER(CStats),
                                    C.POINTER(CLogRow), _I64]),
+    "culamp_probe_pipes": (C.c_int, [_VP, C.POINTER(_D), _VP]),
     "culamp_marginal_error_fp64": (C.c_int, [_VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, _VP, _VP,
                                              _D, _D, _D, C.POINTER(_D), C.POINTER(_D), _VP]),
 }

@@ -1,0 +1,165 @@
+# CuLAMPB200.jl -- Julia ccall layer over libculamp_b200 (include/culamp.h).
+#
+# Drop-in for the kernelized path of CuLAMP.jl: the functions below keep the
+# reference's names and signatures (src/solvers/SinkhornKernel.jl:477-489,
+# src/solvers/MirrorProxKernel.jl:1019, src/solvers/AnnealedSinkhorn.jl:149-160)
+# and forward device pointers of CuArray{Float64} to the C ABI. A 3 x N
+# column-major CuArray has the point-major layout the library expects.
+#
+# Julia is not installed in the environment this library was built in, so this
+# file has not been executed; it is the binding a maintainer adds next to
+# CuLAMP.jl (see INTEGRATION.md).
+module CuLAMPB200
+
+using CUDA
+
+const libculamp = joinpath(@__DIR__, "..", "libculamp_b200.so")
+
+const CULAMP_FLAG_TRUE_PINF = UInt32(1)
+const CULAMP_FLAG_CHECK_ALWAYS = UInt32(2)
+const CULAMP_FLAG_MARGINAL_ONLY = UInt32(4)
+const CULAMP_FLAG_FORM_PLAIN = UInt32(8)
+
+# struct culamp_args (EOTArgs, src/Utilities.jl:18-31)
+struct CArgs
+    eta_p::Float64; eta_mu::Float64; tau_p::Float64; tau_mu::Float64
+    alpha::Float64; B::Float64; epsilon::Float64; anneal_mult::Float64
+    itermax::Int64; inner_iter::Int64; tmax::Float64; verbose::Int32; pad::Int32
+end
+CArgs(a) = CArgs(a.eta_p, a.eta_mu, a.tau_p, a.tau_mu, a.alpha, a.B, Float64(a.epsilon),
+                 a.anneal_mult, a.itermax, a.inner_iter, a.tmax, Int32(a.verbose), Int32(0))
+
+struct CLogRow
+    time_s::Float64; iter::Float64; infeas::Float64; ot_objective::Float64; primal::Float64; dual::Float64
+end
+
+mutable struct CStats
+    iterations::Int64; num_iter::Int64; residual::Float64; objective::Float64; winf::Float64
+    eta_t::Float64; s_t::Float64; elapsed_ms::Float64; log_rows::Int64; stopped::Int32; status::Int32
+    CStats() = new(0, 0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0, 0, 0)
+end
+
+const _handle = Ref{Ptr{Cvoid}}(C_NULL)
+
+function handle()
+    if _handle[] == C_NULL
+        h = Ref{Ptr{Cvoid}}(C_NULL)
+        st = ccall((:culamp_create, libculamp), Cint, (Ptr{Ptr{Cvoid}}, Cint), h, CUDA.device().handle)
+        st == 0 || error("culamp_create failed with status $st")
+        _handle[] = h[]
+    end
+    return _handle[]
+end
+
+function check(st)
+    if st != 0
+        msg = unsafe_string(ccall((:culamp_last_error, libculamp), Cstring, (Ptr{Cvoid},), handle()))
+        error("culamp status $st: $msg")
+    end
+end
+
+stream_ptr() = reinterpret(Ptr{Cvoid}, CUDA.stream().handle)
+
+"""
+    sinkhorn_color_transfer(img1, img2, marginal1, marginal2, args, frequency=100, p=2;
+                            return_cuda=false, return_assignments=true, φ0=nothing, ψ0=nothing)
+
+SinkhornKernel.jl:477-559 on libculamp_b200.
+"""
+function sinkhorn_color_transfer(img1::CuArray{Float64}, img2::CuArray{Float64},
+                                 marginal1::CuArray{Float64}, marginal2::CuArray{Float64},
+                                 args, frequency::Int=100, p::Union{Int,Float64}=2;
+                                 return_cuda::Bool=false, return_assignments::Bool=true,
+                                 φ0=nothing, ψ0=nothing, flags::UInt32=UInt32(0))
+    d, N = size(img1)
+    M = size(img2, 2)
+    φ = CUDA.zeros(Float64, N)
+    ψ = CUDA.zeros(Float64, M)
+    stats = CStats()
+    cargs = Ref(CArgs(args))
+    logbuf = Vector{CLogRow}(undef, 100_000)
+    st = ccall((:culamp_sinkhorn, libculamp), Cint,
+               (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Int64, Int64, Int32, CuPtr{Float64},
+                CuPtr{Float64}, Ptr{CArgs}, Int64, Float64, CuPtr{Float64}, CuPtr{Float64}, UInt32,
+                CuPtr{Float64}, CuPtr{Float64}, Ref{CStats}, Ptr{CLogRow}, Int64, Ptr{Cvoid}),
+               handle(), img1, img2, N, M, d, marginal1, marginal2, cargs, frequency, Float64(p),
+               isnothing(φ0) ? CU_NULL : pointer(φ0), isnothing(ψ0) ? CU_NULL : pointer(ψ0), flags,
+               φ, ψ, stats, logbuf, length(logbuf), stream_ptr())
+    check(st)
+    if args.verbose
+        println("time(s),iter,infeas,ot_objective,dual")
+        for r in logbuf[1:stats.log_rows]
+            @printf "%.6e,%d,%.14e,%.14e,%.14e,sinkhorn_kernel\n" r.time_s Int(r.iter) r.infeas r.ot_objective r.dual
+        end
+    end
+    if !return_assignments
+        return_cuda && return φ, ψ, stats.objective, stats.residual, stats.num_iter
+        return Array(φ), Array(ψ), stats.objective, stats.residual
+    end
+    out1 = similar(img1); out2 = similar(img2)
+    cp = p == 1 ? 1.0 : 2.0   # the reference's barycentric map cost (SinkhornKernel.jl:146-150)
+    check(ccall((:culamp_barycentric_sk, libculamp), Cint,
+                (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, CuPtr{Float64}, Int64, Int64, Int32,
+                 CuPtr{Float64}, CuPtr{Float64}, Float64, Float64, Float64, Ptr{Cvoid}),
+                handle(), out1, img1, img2, N, M, d, φ, ψ, args.eta_p, stats.winf, cp, stream_ptr()))
+    check(ccall((:culamp_barycentric_sk, libculamp), Cint,
+                (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, CuPtr{Float64}, Int64, Int64, Int32,
+                 CuPtr{Float64}, CuPtr{Float64}, Float64, Float64, Float64, Ptr{Cvoid}),
+                handle(), out2, img2, img1, M, N, d, ψ, φ, args.eta_p, stats.winf, cp, stream_ptr()))
+    return Array(φ), Array(ψ), Array(out1), Array(out2)
+end
+
+"""
+    extragradient_color_transfer(img1, img2, marginal1, marginal2, args, frequency=100, p=2.0)
+
+MirrorProxKernel.jl:1019-1132 (LAMP) on libculamp_b200; returns (ν, φ, ψ).
+"""
+function extragradient_color_transfer(img1::CuArray{Float64}, img2::CuArray{Float64},
+                                      marginal1::CuArray{Float64}, marginal2::CuArray{Float64},
+                                      args, frequency::Int=100, p::Float64=2.0; flags::UInt32=UInt32(0))
+    d, N = size(img1)
+    M = size(img2, 2)
+    ν = CUDA.zeros(Float64, M); φ = CUDA.zeros(Float64, N)
+    ψ = CUDA.zeros(Float64, M); θ = CUDA.zeros(Float64, M)
+    stats = CStats()
+    cargs = Ref(CArgs(args))
+    logbuf = Vector{CLogRow}(undef, 100_000)
+    check(ccall((:culamp_lamp, libculamp), Cint,
+                (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Int64, Int64, Int32, CuPtr{Float64},
+                 CuPtr{Float64}, Ptr{CArgs}, Int64, Float64, UInt32, CuPtr{Float64}, CuPtr{Float64},
+                 CuPtr{Float64}, CuPtr{Float64}, Ref{CStats}, Ptr{CLogRow}, Int64, Ptr{Cvoid}),
+                handle(), img1, img2, N, M, d, marginal1, marginal2, cargs, frequency, p, flags,
+                ν, φ, ψ, θ, stats, logbuf, length(logbuf), stream_ptr()))
+    return Array(ν), Array(φ), Array(ψ)
+end
+
+"""
+    annealed_sinkhorn_euclidean(marginal1, marginal2, location1, location2, out1, out2,
+                                potentials, args, frequency, p)
+
+AnnealedSinkhorn.jl:149-261 on libculamp_b200 (potentials file output kept).
+"""
+function annealed_sinkhorn_euclidean(marginal1::CuArray{Float64}, marginal2::CuArray{Float64},
+                                     location1::CuArray{Float64}, location2::CuArray{Float64},
+                                     out1::String, out2::String, potentials::String, args,
+                                     frequency::Int, p)
+    d, N = size(location1)
+    M = size(location2, 2)
+    φ = CUDA.zeros(Float64, N); ψ = CUDA.zeros(Float64, M)
+    stats = CStats()
+    cargs = Ref(CArgs(args))
+    check(ccall((:culamp_annealed_sinkhorn, libculamp), Cint,
+                (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Int64, Int64, Int32, CuPtr{Float64},
+                 CuPtr{Float64}, Ptr{CArgs}, Int64, Float64, UInt32, CuPtr{Float64}, CuPtr{Float64},
+                 Ref{CStats}, Ptr{CLogRow}, Int64, Ptr{Cvoid}),
+                handle(), location1, location2, N, M, d, marginal1, marginal2, cargs, frequency,
+                Float64(p), UInt32(0), φ, ψ, stats, C_NULL, 0, stream_ptr()))
+    φ_out, ψ_out = Array(φ), Array(ψ)
+    if potentials != ""
+        open(potentials * ".row", "w") do f; foreach(v -> println(f, v), φ_out); end
+        open(potentials * ".col", "w") do f; foreach(v -> println(f, v), ψ_out); end
+    end
+    return φ_out, ψ_out, stats.objective
+end
+
+end # module

@@ -207,6 +207,12 @@ int culamp_marginal_error_fp64(culamp_handle h, const double *x, const double *y
                                const double *phi, const double *psi, double reg, double winf,
                                double p, double *row_l1, double *col_l1, void *stream);
 
+/* ------------------------------------------------------------ diagnostics
+ * No counterpart in the reference. Measures, on the running GPU, the sustained
+ * instruction rates that bound the pair passes: out[0] = DFMA/s, out[1] = MUFU
+ * ex2/s, out[2] = FP64->FP32 conversions/s, out[3] = SM count. Synchronous. */
+int culamp_probe_pipes(culamp_handle h, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

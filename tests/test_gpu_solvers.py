@@ -2,8 +2,9 @@
 committed golden fixtures: same iteration counts / stopping iteration, same
 convergence-log rows, potentials and objectives within tolerance.
 
-Tolerances: potentials 2e-6 absolute (natural-log units, FP32-exp form),
-residuals / objectives 1e-5 relative, eta_t bit-exact.
+Tolerances: Sinkhorn potentials 2e-6 absolute (natural-log units, FP32-exp
+form); LAMP averaged potentials nu 2e-6 and theta 5e-6 absolute (|theta| < 1);
+residuals / objectives 1e-5 relative; eta_t bit-exact.
 """
 import math
 import os
@@ -70,8 +71,8 @@ def test_lamp_matches_golden(grid8, eta_tag, eta_p, p):
     st = g[pre + "_stats"]
     assert res.iterations == st[0]
     assert res.eta_t == st[4]                                 # bit-exact recursion
-    np.testing.assert_allclose(res.nu, g[pre + "_nu"], atol=1e-7)
-    np.testing.assert_allclose(res.theta, g[pre + "_theta"], atol=1e-6)
+    np.testing.assert_allclose(res.nu, g[pre + "_nu"], atol=2e-6)
+    np.testing.assert_allclose(res.theta, g[pre + "_theta"], atol=5e-6)
     np.testing.assert_allclose(res.phi, g[pre + "_phi"], atol=POT_ATOL * max(1.0, 1.0 / st[4] * 1e-4))
     assert res.residual == pytest.approx(st[1], rel=1e-3, abs=1e-8)
     assert res.objective == pytest.approx(st[2], rel=REL)
@@ -105,8 +106,8 @@ def test_ragged_solvers(golden_dir):
     assert res.objective == pytest.approx(g["sk_stats"][1], rel=REL)
     b = cb.EOTArgs(eta_p=5e-2, epsilon=0.0, itermax=80, verbose=False, B=1.1)
     lr = cb.solve_lamp(g["x"], g["y"], g["r"], g["c"], b, frequency=50, p=2.0)
-    np.testing.assert_allclose(lr.nu, g["lamp_nu"], atol=1e-7)
-    np.testing.assert_allclose(lr.theta, g["lamp_theta"], atol=1e-6)
+    np.testing.assert_allclose(lr.nu, g["lamp_nu"], atol=2e-6)
+    np.testing.assert_allclose(lr.theta, g["lamp_theta"], atol=5e-6)
     assert lr.eta_t == g["lamp_stats"][3]
 
 
