@@ -150,4 +150,40 @@ static __global__ void setup_reduce_kernel(double *out, const double *v, long lo
     if (threadIdx.x == 0) { out[0] = s0[0]; out[1] = s1[0]; out[2] = s2[0]; }
 }
 
+// Per-dimension [min, max] over the union of two point clouds: block k reduces
+// dimension k. out[2k] = min, out[2k+1] = max.
+static __global__ void dim_range_kernel(double *out, const double *x, long long n, const double *y,
+                                        long long m, int d) {
+    __shared__ double smn[256], smx[256];
+    const int k = blockIdx.x;
+    double mn = INFINITY, mx = -INFINITY;
+    for (long long i = threadIdx.x; i < n + m; i += blockDim.x) {
+        const double v = i < n ? x[i * d + k] : y[(i - n) * d + k];
+        mn = fmin(mn, v);
+        mx = fmax(mx, v);
+    }
+    smn[threadIdx.x] = mn;
+    smx[threadIdx.x] = mx;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            smn[threadIdx.x] = fmin(smn[threadIdx.x], smn[threadIdx.x + o]);
+            smx[threadIdx.x] = fmax(smx[threadIdx.x], smx[threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { out[2 * k] = smn[0]; out[2 * k + 1] = smx[0]; }
+}
+
+// out[i*dk + q] = in[i*d + keep[q]] for the kept dimensions (keep given by value).
+struct DimKeep { int idx[64]; };
+static __global__ void gather_dims_kernel(double *out, const double *in, long long n, int d, int dk,
+                                          DimKeep keep) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= n * dk) return;
+    const long long i = t / dk;
+    const int q = (int)(t - i * dk);
+    out[t] = in[i * d + keep.idx[q]];
+}
+
 }  // namespace culamp_dev

@@ -161,7 +161,7 @@ int ensure_solver(culamp_handle h, int n, int m, int d, int64_t log_cap) {
     R(S.prev_phi, nm * sizeof(double));
     R(S.prev_psi, nm * sizeof(double));
     R(S.ctl, sizeof(Ctl), true);
-    R(S.setup, 8 * sizeof(double));
+    R(S.setup, (8 + 2 * MAXD) * sizeof(double));
     R(S.logbuf, (size_t)(log_cap > 1 ? log_cap : 1) * sizeof(culamp_log_row));
     // scratch for both pass orientations
     LaunchShape a = pass_shape(n, m, d, ACC_LSE, h->sm_count);
@@ -256,25 +256,45 @@ int check_solver_args(culamp_handle h, const double *x, const double *y, int64_t
     return CULAMP_OK;
 }
 
-// Copy user inputs into the workspace, validate marginals (positive, finite).
+// Copy user inputs into the workspace and validate the marginals (positive,
+// finite). Coordinates that are the same for every point of both clouds add
+// exactly 0 to every cost (for p = 1, 2, Inf and any p > 0), so those
+// dimensions are dropped: *d_eff receives the kept dimension count (>= 1).
 int stage_inputs(culamp_handle h, const double *x, const double *y, int n, int m, int d,
-                 const double *r, const double *c, cudaStream_t st, double *hr_out) {
+                 const double *r, const double *c, cudaStream_t st, double *hr_out, int *d_eff) {
     Solver &S = *h->solver;
-    CUDA_TRY(h, cudaMemcpyAsync(S.X.ptr, x, (size_t)n * d * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    CUDA_TRY(h, cudaMemcpyAsync(S.Y.ptr, y, (size_t)m * d * sizeof(double), cudaMemcpyDeviceToDevice, st));
     CUDA_TRY(h, cudaMemcpyAsync(S.r.ptr, r, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     CUDA_TRY(h, cudaMemcpyAsync(S.c.ptr, c, (size_t)m * sizeof(double), cudaMemcpyDeviceToDevice, st));
     double *su = S.setup.as<double>();
     setup_reduce_kernel<<<1, 256, 0, st>>>(su, S.r.as<double>(), n);
     setup_reduce_kernel<<<1, 256, 0, st>>>(su + 3, S.c.as<double>(), m);
+    dim_range_kernel<<<d, 256, 0, st>>>(su + 8, x, n, y, m, d);
     CUDA_TRY(h, cudaGetLastError());
-    double hv[6];
-    CUDA_TRY(h, cudaMemcpyAsync(hv, su, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    double hv[8 + 2 * MAXD];
+    CUDA_TRY(h, cudaMemcpyAsync(hv, su, (8 + 2 * (size_t)d) * sizeof(double), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(h, cudaStreamSynchronize(st));
     if (!(hv[1] > 0.0) || !(hv[4] > 0.0) || !std::isfinite(hv[2]) || !std::isfinite(hv[5]))
         return culamp_set_error(h, CULAMP_ERR_INVALID_ARG,
                                 "marginals must be positive and finite (min r=%g, min c=%g)", hv[1], hv[4]);
+    DimKeep keep;
+    int dk = 0;
+    for (int k = 0; k < d; ++k) {
+        const double lo = hv[8 + 2 * k], hi = hv[8 + 2 * k + 1];
+        if (!std::isfinite(lo) || !std::isfinite(hi))
+            return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "non-finite coordinate in dimension %d", k);
+        if (hi > lo) keep.idx[dk++] = k;
+    }
+    if (dk == 0) keep.idx[dk++] = 0;
+    if (dk == d) {
+        CUDA_TRY(h, cudaMemcpyAsync(S.X.ptr, x, (size_t)n * d * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(h, cudaMemcpyAsync(S.Y.ptr, y, (size_t)m * d * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    } else {
+        gather_dims_kernel<<<(unsigned)(((long long)n * dk + 255) / 256), 256, 0, st>>>(S.X.as<double>(), x, n, d, dk, keep);
+        gather_dims_kernel<<<(unsigned)(((long long)m * dk + 255) / 256), 256, 0, st>>>(S.Y.as<double>(), y, m, d, dk, keep);
+        CUDA_TRY(h, cudaGetLastError());
+    }
     if (hr_out) *hr_out = hv[0];
+    *d_eff = dk;
     return CULAMP_OK;
 }
 
@@ -474,8 +494,10 @@ extern "C" int culamp_sinkhorn(culamp_handle h, const double *x, const double *y
     s = ensure_solver(h, (int)n, (int)m, d, log ? log_cap : 0);
     if (s) return s;
     Solver &S = *h->solver;
-    s = stage_inputs(h, x, y, (int)n, (int)m, d, r, c, st, nullptr);
+    int dk = d;
+    s = stage_inputs(h, x, y, (int)n, (int)m, d, r, c, st, nullptr, &dk);
     if (s) return s;
+    d = dk;
     if (phi0) CUDA_TRY(h, cudaMemcpyAsync(S.phi.ptr, phi0, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     else CUDA_TRY(h, cudaMemsetAsync(S.phi.ptr, 0, n * sizeof(double), st));
     if (psi0) CUDA_TRY(h, cudaMemcpyAsync(S.psi.ptr, psi0, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -611,8 +633,10 @@ extern "C" int culamp_lamp(culamp_handle h, const double *x, const double *y, in
     if (s) return s;
     Solver &S = *h->solver;
     double sum_rlogr = 0.0;
-    s = stage_inputs(h, x, y, (int)n, (int)m, d, r, c, st, &sum_rlogr);
+    int dk = d;
+    s = stage_inputs(h, x, y, (int)n, (int)m, d, r, c, st, &sum_rlogr, &dk);
     if (s) return s;
+    d = dk;
     double winf = 0.0;
     s = compute_winf(h, (int)n, (int)m, d, p, st, &winf);
     if (s) return s;
@@ -759,8 +783,10 @@ extern "C" int culamp_annealed_sinkhorn(culamp_handle h, const double *x, const 
     s = ensure_solver(h, (int)n, (int)m, d, 0);
     if (s) return s;
     Solver &S = *h->solver;
-    s = stage_inputs(h, x, y, (int)n, (int)m, d, r, c, st, nullptr);
+    int dk = d;
+    s = stage_inputs(h, x, y, (int)n, (int)m, d, r, c, st, nullptr, &dk);
     if (s) return s;
+    d = dk;
     double winf = 0.0;
     s = compute_winf(h, (int)n, (int)m, d, p, st, &winf);
     if (s) return s;

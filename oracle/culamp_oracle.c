@@ -438,6 +438,7 @@ int or_annealed_sinkhorn_kernel(const double *x, const double *y, int64_t n, int
         a.eta_p = eta;
         or_sinkhorn_kernel(x, y, n, m, d, r, c, &a, frequency, p, phiws, psiws, flags, phi, psi,
                            &inner, NULL, 0);
+        st->iterations += 1; /* stages run */
         total_iters += inner.num_iter;
         double el = now_s() - t0;
         a.tmax = tmax - el;
@@ -453,7 +454,6 @@ int or_annealed_sinkhorn_kernel(const double *x, const double *y, int64_t n, int
         memcpy(psiprev, psi, sizeof(double) * (size_t)m);
         preveta = eta;
         eta = q * eta > eta_final ? q * eta : eta_final;
-        st->iterations += 1; /* stages completed before the last */
     }
     st->num_iter = total_iters;
     free(phiws); free(psiws); free(phiprev); free(psiprev);
