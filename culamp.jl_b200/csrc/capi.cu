@@ -245,7 +245,7 @@ PassParams base_params(const double *X, const double *Y, int n, int m, int d, do
 }
 
 int run_pass(culamp_handle h, PassParams P, int pm, int acc, cudaStream_t st) {
-    LaunchShape sh = pass_shape(P.n, P.m, P.d, acc, h->sm_count);
+    LaunchShape sh = pass_shape(P.n, P.m, P.d, acc, h->sm_count, P.want_moment != 0);
     cudaError_t e = h->scratch.reserve(sh.part_bytes, (size_t)sh.rb);
     if (e != cudaSuccess)
         return culamp_set_error(h, CULAMP_ERR_ALLOC, "scratch: %s", cudaGetErrorString(e));

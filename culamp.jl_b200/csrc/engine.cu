@@ -14,11 +14,15 @@ int pmode_of(double p) {
     return P_GEN;
 }
 
-LaunchShape pass_shape(int n, int m, int d, int acc, int sm_count) {
+LaunchShape pass_shape(int n, int m, int d, int acc, int sm_count, bool mom) {
     LaunchShape s{};
-    s.rb = (n + ROWS - 1) / ROWS;
-    if (s.rb < 1) s.rb = 1;
     const bool packed = d >= 1 && d <= MAXD_PACKED;
+    // 8 rows per thread amortise each broadcast column over more pairs; used
+    // when there are enough row blocks to fill the GPU with few column splits.
+    s.R = (acc == ACC_LSE && packed && !mom && n >= 16384) ? RPT_BIG : RPT;
+    const int rows = TPB * s.R;
+    s.rb = (n + rows - 1) / rows;
+    if (s.rb < 1) s.rb = 1;
     const int ch = packed ? CHUNK : CHUNK_G;
     // Aim for ~4 resident CTAs per SM over the whole grid; never split below one tile.
     const int target = 4 * (sm_count > 0 ? sm_count : 148);
@@ -39,9 +43,9 @@ LaunchShape pass_shape(int n, int m, int d, int acc, int sm_count) {
     return s;
 }
 
-template <int PM, int D, int ACC>
+template <int PM, int D, int ACC, int R, bool MOM>
 static cudaError_t launch_t(const PassParams &P, const LaunchShape &sh, cudaStream_t st) {
-    auto kern = pair_pass_kernel<PM, D, ACC>;
+    auto kern = pair_pass_kernel<PM, D, ACC, R, MOM>;
     if (sh.smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)sh.smem);
@@ -52,13 +56,23 @@ static cudaError_t launch_t(const PassParams &P, const LaunchShape &sh, cudaStre
     return cudaGetLastError();
 }
 
+template <int PM, int D, int ACC>
+static cudaError_t launch_v(const PassParams &P, const LaunchShape &sh, cudaStream_t st) {
+    if constexpr (ACC == ACC_LSE) {
+        if (P.want_moment) return launch_t<PM, D, ACC, RPT, true>(P, sh, st);
+        if constexpr (D > 0)
+            if (sh.R == RPT_BIG) return launch_t<PM, D, ACC, RPT_BIG, false>(P, sh, st);
+    }
+    return launch_t<PM, D, ACC, RPT, false>(P, sh, st);
+}
+
 template <int PM, int ACC>
 static cudaError_t launch_d(const PassParams &P, const LaunchShape &sh, cudaStream_t st) {
     switch (P.d) {
-        case 1: return launch_t<PM, 1, ACC>(P, sh, st);
-        case 2: return launch_t<PM, 2, ACC>(P, sh, st);
-        case 3: return launch_t<PM, 3, ACC>(P, sh, st);
-        default: return launch_t<PM, 0, ACC>(P, sh, st);
+        case 1: return launch_v<PM, 1, ACC>(P, sh, st);
+        case 2: return launch_v<PM, 2, ACC>(P, sh, st);
+        case 3: return launch_v<PM, 3, ACC>(P, sh, st);
+        default: return launch_v<PM, 0, ACC>(P, sh, st);
     }
 }
 
@@ -74,6 +88,7 @@ static cudaError_t launch_p(const PassParams &P, int pm, const LaunchShape &sh, 
 
 cudaError_t launch_pass(PassParams P, int pm, int acc, const LaunchShape &sh, Scratch &scr,
                         cudaStream_t st) {
+    if (P.want_moment && sh.R != RPT) return cudaErrorInvalidValue;   // shape built without mom
     P.splits = sh.splits;
     P.cols_per_split = sh.cols_per_split;
     P.part = scr.part.as<double>();

@@ -39,8 +39,9 @@
 namespace culamp_dev {
 
 constexpr int TPB = 128;          // threads per CTA
-constexpr int RPT = 2;            // output rows per thread
-constexpr int ROWS = TPB * RPT;   // output rows per CTA
+constexpr int RPT = 2;            // output rows per thread, small-problem / generic variants
+constexpr int RPT_BIG = 8;        // output rows per thread, packed log-sum-exp variant
+constexpr int ROWS = TPB * RPT;   // output rows per CTA (RPT variant)
 constexpr int CHUNK = 256;        // columns per shared-memory tile (d <= 3)
 constexpr int KC = 4;             // columns per online-max sub-chunk
 constexpr int MAXD_PACKED = 3;    // packed fast path: d <= 3
@@ -85,7 +86,7 @@ enum Finish {
 };
 
 // Gate: when the kernel runs.
-enum Gate { GATE_ALWAYS = 0, GATE_CHECK = 1 };
+enum Gate { GATE_ALWAYS = 0, GATE_CHECK = 1, GATE_NOCHECK = 2 };
 
 // Device-resident solver state. All fields written by device code are read by
 // later kernels only (stream order), never by concurrently running CTAs.
@@ -143,7 +144,7 @@ struct PassParams {
     const double *cvec, *eta_mu_i;
     double eta_mu_exp, minv, maxv;
     // moments
-    int want_moment;            // 0 never, 1 always, 2 when ctl->do_check
+    int want_moment;            // 1: accumulate the softmax-weighted cost moment (MOM kernels)
     // gating and control
     int gate;
     int finish;
@@ -587,8 +588,141 @@ __device__ __forceinline__ double block_max1(double x, double *red) {
     return x;
 }
 
-template <int PM, int D, int ACC>
-__global__ void __launch_bounds__(TPB) pair_pass_kernel(PassParams P) {
+__device__ __forceinline__ void kahan_add(float &s, float &c, float v) {
+    const float y = v - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+}
+
+// One column against R register-resident rows (packed d <= 3 log-sum-exp path).
+// t = exponent in log2 units (FP64); f = t - M rounded to FP32; a new running
+// max rescales the row's sums; e = 2^f on the MUFU pipe goes into an 8-term
+// FP32 chunk sum (merged into a Kahan-compensated total every 8 columns).
+template <int PM, int D, int R, bool MOM>
+__device__ __forceinline__ void lse_step(const double4 col, const double (&xr)[R][D],
+                                         const double (&xs)[(PM == P_SQ && MOM) ? R : 1][D],
+                                         double a2, double pexp, double (&M)[R], float (&S)[R],
+                                         float (&Cc)[R], float (&cs)[R], float (&mo)[R]) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        double t;
+        float cf = 0.f;
+        if (PM == P_SQ) {
+            t = col.w;
+            if (D >= 3) t = fma(xr[r][D >= 3 ? 2 : 0], col.z, t);
+            if (D >= 2) t = fma(xr[r][D >= 2 ? 1 : 0], col.y, t);
+            t = fma(xr[r][0], col.x, t);
+            if (MOM) {
+                const double yv[3] = {col.x, col.y, col.z};
+                double cc = 0.0;
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+                    const double df = xs[(PM == P_SQ && MOM) ? r : 0][k] - yv[k];
+                    cc = fma(df, df, cc);
+                }
+                cf = (float)cc;
+            }
+        } else {
+            const double yv[3] = {col.x, col.y, col.z};
+            const double cc = pair_cost_direct<PM>(xr[r], yv, D, pexp);
+            t = fma(cc, a2, col.w);
+            if (MOM) cf = (float)cc;
+        }
+        float f = (float)(t - M[r]);
+        if (f > 0.f) {
+            const float sc = ex2_approx(-f);
+            S[r] *= sc;
+            Cc[r] *= sc;
+            cs[r] *= sc;
+            if (MOM) mo[r] *= sc;
+            M[r] = t;
+            f = 0.f;
+        }
+        const float e = ex2_approx(f);
+        cs[r] += e;
+        if (MOM) mo[r] = fmaf(e, cf, mo[r]);
+    }
+}
+
+// Packed (d <= 3) log-sum-exp tile: rows in registers, column tiles of CHUNK
+// (y - ctr, g) double4 entries in shared memory, broadcast to the warp.
+template <int PM, int D, int R, bool MOM>
+__device__ __forceinline__ void tile_lse_packed(const PassParams &P, double alpha, double beta,
+                                                int row_base, int cbeg, int cend, double *smem,
+                                                double (&Mo)[R], double (&So)[R],
+                                                double (&MOMo)[R], double (&Ho)[R]) {
+    constexpr bool SQ = (PM == P_SQ);
+    const int tid = threadIdx.x;
+    const double a2 = alpha * LOG2E;
+    const double cb = P.colpot_unit ? LOG2E : beta * LOG2E;
+    double ctr[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) ctr[k] = P.ctr ? P.ctr[k] : 0.0;
+    double xr[R][D];
+    double xs[(SQ && MOM) ? R : 1][D];
+    double M[R];
+    float S[R], Cc[R], cs[R], mo[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int row = row_base + tid + r * TPB;
+        const bool ok = row < P.n;
+        double h = 0.0;
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            const double v = ok ? P.X[(size_t)row * D + k] - ctr[k] : 0.0;
+            xr[r][k] = SQ ? -2.0 * a2 * v : v;
+            if (SQ && MOM) xs[(SQ && MOM) ? r : 0][k] = v;
+            h = fma(v, v, h);
+        }
+        Ho[r] = SQ ? a2 * h : 0.0;
+        M[r] = -1e300;   // finite: an all -inf row keeps S = 0 without NaN
+        S[r] = 0.f; Cc[r] = 0.f; cs[r] = 0.f; mo[r] = 0.f;
+    }
+    double4 *tile = reinterpret_cast<double4 *>(smem);
+    for (int c0 = cbeg; c0 < cend; c0 += CHUNK) {
+        __syncthreads();
+        for (int q = tid; q < CHUNK; q += TPB) {
+            const int j = c0 + q;
+            double4 v = make_double4(0.0, 0.0, 0.0, -INFINITY);
+            if (j < cend) {
+                double yy[3] = {0.0, 0.0, 0.0};
+                double s2 = 0.0;
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+                    yy[k] = P.Y[(size_t)j * D + k] - ctr[k];
+                    s2 = fma(yy[k], yy[k], s2);
+                }
+                const double pot = P.colpot ? P.colpot[j] : 0.0;
+                double g = (cb == 0.0) ? 0.0 : cb * pot;
+                if (SQ) g += a2 * s2;
+                v = make_double4(yy[0], yy[1], yy[2], g);
+            }
+            tile[q] = v;
+        }
+        __syncthreads();
+        const int nc = min(CHUNK, cend - c0);
+        int q = 0;
+        for (; q + 8 <= nc; q += 8) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) lse_step<PM, D, R, MOM>(tile[q + u], xr, xs, a2, P.pexp, M, S, Cc, cs, mo);
+#pragma unroll
+            for (int r = 0; r < R; ++r) { kahan_add(S[r], Cc[r], cs[r]); cs[r] = 0.f; }
+        }
+        for (; q < nc; ++q) lse_step<PM, D, R, MOM>(tile[q], xr, xs, a2, P.pexp, M, S, Cc, cs, mo);
+#pragma unroll
+        for (int r = 0; r < R; ++r) { kahan_add(S[r], Cc[r], cs[r]); cs[r] = 0.f; }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        Mo[r] = M[r];
+        So[r] = (double)S[r] - (double)Cc[r];
+        MOMo[r] = (double)mo[r];
+    }
+}
+
+template <int PM, int D, int ACC, int R, bool MOM>
+__global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassParams P) {
     extern __shared__ __align__(16) double smem[];
     __shared__ double red[4 * (TPB / 32)];
     __shared__ int s_last;
@@ -596,27 +730,29 @@ __global__ void __launch_bounds__(TPB) pair_pass_kernel(PassParams P) {
     if (ctl) {
         if (ctl->stop) return;
         if (P.gate == GATE_CHECK && !ctl->do_check) return;
+        if (P.gate == GATE_NOCHECK && ctl->do_check) return;
     }
     double alpha = 0.0, beta = 0.0;
     if (ACC == ACC_LSE) resolve_coefs(P, alpha, beta);
-    const bool mom = (P.want_moment == 1) || (P.want_moment == 2 && ctl && ctl->do_check);
 
     const int rb = blockIdx.x;               // row block
     const int sp = blockIdx.y;               // column split
-    const int row_base = rb * ROWS;
+    const int row_base = rb * (TPB * R);
     const int cbeg = sp * P.cols_per_split;
     const int cend = min(P.m, cbeg + P.cols_per_split);
 
-    double Mv[RPT], Sv[RPT], MOMv[RPT], Hv[RPT];
-    if (ACC == ACC_LSE && mom)
-        tile_reduce<PM, D, ACC, true>(P, alpha, beta, row_base, cbeg, cend, smem, Mv, Sv, MOMv, Hv);
-    else
-        tile_reduce<PM, D, ACC, false>(P, alpha, beta, row_base, cbeg, cend, smem, Mv, Sv, MOMv, Hv);
+    double Mv[R], Sv[R], MOMv[R], Hv[R];
+    if constexpr (ACC == ACC_LSE && D > 0) {
+        tile_lse_packed<PM, D, R, MOM>(P, alpha, beta, row_base, cbeg, cend, smem, Mv, Sv, MOMv, Hv);
+    } else {
+        static_assert(R == RPT, "generic / min-max tiles use RPT rows per thread");
+        tile_reduce<PM, D, ACC, MOM>(P, alpha, beta, row_base, cbeg, cend, smem, Mv, Sv, MOMv, Hv);
+    }
 
     if (P.splits > 1) {
         // publish partials, take a ticket; the last CTA of this row block merges
 #pragma unroll
-        for (int r = 0; r < RPT; ++r) {
+        for (int r = 0; r < R; ++r) {
             const int row = row_base + threadIdx.x + r * TPB;
             if (row < P.n) {
                 double *pp = P.part + ((size_t)sp * P.n + row) * 3;
@@ -633,7 +769,7 @@ __global__ void __launch_bounds__(TPB) pair_pass_kernel(PassParams P) {
         if (!s_last) return;
         __threadfence();
 #pragma unroll
-        for (int r = 0; r < RPT; ++r) {
+        for (int r = 0; r < R; ++r) {
             const int row = row_base + threadIdx.x + r * TPB;
             if (row >= P.n) continue;
             double M = (ACC == ACC_MIN) ? INFINITY : -INFINITY, S = 0.0, MO = 0.0;
@@ -656,7 +792,7 @@ __global__ void __launch_bounds__(TPB) pair_pass_kernel(PassParams P) {
     if (P.lamp_step == LAMP_A) { double sn; lamp_next(ctl->eta_t, ctl->s_t, ctl->tau_p, ctl->eta_lamp, en, sn); }
     else if (P.lamp_step == LAMP_B) en = ctl->eta_next;
 #pragma unroll
-    for (int r = 0; r < RPT; ++r) {
+    for (int r = 0; r < R; ++r) {
         const int o = row_base + threadIdx.x + r * TPB;
         if (o >= P.n) continue;
         if (ACC != ACC_LSE) {

@@ -56,6 +56,7 @@ struct Scratch {
 };
 
 struct LaunchShape {
+    int R;             // output rows per thread (RPT or RPT_BIG)
     int rb;            // row blocks
     int splits;        // column splits
     int cols_per_split;
@@ -64,7 +65,8 @@ struct LaunchShape {
 };
 
 // Grid and scratch requirement of a pass over n output rows and m columns.
-LaunchShape pass_shape(int n, int m, int d, int acc, int sm_count);
+// `mom`: the pass accumulates the cost moment (selects the RPT variant).
+LaunchShape pass_shape(int n, int m, int d, int acc, int sm_count, bool mom = false);
 
 // Launch one pair pass. The scratch must already hold pass_shape(...) bytes
 // (so the call is legal inside stream capture).

@@ -164,10 +164,14 @@ int ensure_solver(culamp_handle h, int n, int m, int d, int64_t log_cap) {
     R(S.setup, (8 + 2 * MAXD) * sizeof(double));
     R(S.logbuf, (size_t)(log_cap > 1 ? log_cap : 1) * sizeof(culamp_log_row));
     // scratch for both pass orientations
-    LaunchShape a = pass_shape(n, m, d, ACC_LSE, h->sm_count);
-    LaunchShape b = pass_shape(m, n, d, ACC_LSE, h->sm_count);
-    const size_t pb = a.part_bytes > b.part_bytes ? a.part_bytes : b.part_bytes;
-    const size_t nrb = (size_t)(a.rb > b.rb ? a.rb : b.rb);
+    size_t pb = 0, nrb = 0;
+    for (int mom = 0; mom < 2; ++mom)
+        for (const LaunchShape &sh : {pass_shape(n, m, d, ACC_LSE, h->sm_count, mom),
+                                      pass_shape(m, n, d, ACC_LSE, h->sm_count, mom),
+                                      pass_shape(n, m, d, ACC_MAX, h->sm_count)}) {
+            pb = sh.part_bytes > pb ? sh.part_bytes : pb;
+            nrb = (size_t)sh.rb > nrb ? (size_t)sh.rb : nrb;
+        }
     if (e == cudaSuccess) e = S.scr.reserve(pb, nrb);
     if (e != cudaSuccess) return culamp_set_error(h, CULAMP_ERR_ALLOC, "workspace: %s", cudaGetErrorString(e));
     if (before != ptrs()) {   // any pointer baked into a cached graph moved
@@ -347,7 +351,7 @@ int copy_log(culamp_handle h, const Ctl &c, culamp_log_row *log, int64_t log_cap
 struct SkPlan {
     PassParams k1, k2, k3;
     int pm_iter, pm_resid;
-    LaunchShape s_rows, s_cols;
+    LaunchShape s_rows, s_cols, s_rows_mom;
 };
 
 SkPlan make_sk_plan(culamp_handle h, int n, int m, int d, double p, uint32_t flags) {
@@ -393,6 +397,7 @@ SkPlan make_sk_plan(culamp_handle h, int n, int m, int d, double p, uint32_t fla
     pl.k3.finish = FIN_SK_CHECK;
     pl.s_rows = pass_shape(n, m, d, ACC_LSE, h->sm_count);
     pl.s_cols = pass_shape(m, n, d, ACC_LSE, h->sm_count);
+    pl.s_rows_mom = pass_shape(n, m, d, ACC_LSE, h->sm_count, true);
     return pl;
 }
 
@@ -419,7 +424,7 @@ int sinkhorn_loop(culamp_handle h, int n, int m, int d, double p, double eta, do
     auto body = [&](cudaStream_t s) -> cudaError_t {
         cudaError_t e = launch_pass(pl.k1, pl.pm_iter, ACC_LSE, pl.s_rows, S.scr, s);
         if (e == cudaSuccess) e = launch_pass(pl.k2, pl.pm_iter, ACC_LSE, pl.s_cols, S.scr, s);
-        if (e == cudaSuccess) e = launch_pass(pl.k3, pl.pm_resid, ACC_LSE, pl.s_rows, S.scr, s);
+        if (e == cudaSuccess) e = launch_pass(pl.k3, pl.pm_resid, ACC_LSE, pl.s_rows_mom, S.scr, s);
         return e;
     };
     CUDA_TRY(h, cudaEventRecord(S.ev0, st));
@@ -465,7 +470,7 @@ int sinkhorn_final(culamp_handle h, int n, int m, int d, double p, double eta, d
     P.alpha = -1.0 / (eta * winf);
     P.beta = 1.0;
     P.finish = FIN_SUMS;
-    CUDA_TRY(h, launch_pass(P, pl.pm_resid, ACC_LSE, pl.s_rows, S.scr, st));
+    CUDA_TRY(h, launch_pass(P, pl.pm_resid, ACC_LSE, pl.s_rows_mom, S.scr, st));
     double sums[4];
     CUDA_TRY(h, cudaMemcpyAsync(sums, h->pass_ctl.as<Ctl>()->sums, sizeof(sums), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(h, cudaStreamSynchronize(st));
@@ -535,10 +540,10 @@ extern "C" int culamp_sinkhorn(culamp_handle h, const double *x, const double *y
 namespace {
 
 struct LampPlan {
-    PassParams k1, k2, kd, k3, k4;
+    PassParams k1, k2, k2m, kd, k3, k4;
     int pm;
     bool dual_min;
-    LaunchShape s_rows, s_cols;
+    LaunchShape s_rows, s_cols, s_rows_min, s_cols_mom;
 };
 
 LampPlan make_lamp_plan(culamp_handle h, int n, int m, int d, double p, double winf, double eta,
@@ -570,7 +575,8 @@ LampPlan make_lamp_plan(culamp_handle h, int n, int m, int d, double p, double w
     pl.k2.cvec = S.c.as<double>();
     pl.k2.out = S.res.as<double>();
     pl.k2.out2 = S.cost.as<double>();
-    pl.k2.want_moment = 2;
+    pl.k2.want_moment = 0;
+    pl.k2.gate = GATE_NOCHECK;
     pl.k2.lamp_step = LAMP_A;
     pl.k2.theta = S.theta.as<double>();
     pl.k2.thetab = S.thetab.as<double>();
@@ -581,6 +587,10 @@ LampPlan make_lamp_plan(culamp_handle h, int n, int m, int d, double p, double w
     pl.k2.minv = minv;
     pl.k2.maxv = maxv;
     pl.k2.finish = FIN_LAMP_A;
+    // the same pass with the cost moment, on check iterations only
+    pl.k2m = pl.k2;
+    pl.k2m.want_moment = 1;
+    pl.k2m.gate = GATE_CHECK;
     // Kd (check iterations): dual value at theta
     pl.dual_min = !(eta > 0.0);
     pl.kd = mk(X, Y, n, m, d, p, ctl);
@@ -607,10 +617,13 @@ LampPlan make_lamp_plan(culamp_handle h, int n, int m, int d, double p, double w
     pl.k4.coef_mode = COEF_SPP_NEXT;
     pl.k4.rowpot = S.nub.as<double>();
     pl.k4.want_moment = 0;
+    pl.k4.gate = GATE_ALWAYS;
     pl.k4.lamp_step = LAMP_B;
     pl.k4.finish = FIN_LAMP_B;
     pl.s_rows = pass_shape(n, m, d, ACC_LSE, h->sm_count);
     pl.s_cols = pass_shape(m, n, d, ACC_LSE, h->sm_count);
+    pl.s_rows_min = pass_shape(n, m, d, ACC_MIN, h->sm_count);
+    pl.s_cols_mom = pass_shape(m, n, d, ACC_LSE, h->sm_count, true);
     return pl;
 }
 
@@ -673,8 +686,10 @@ extern "C" int culamp_lamp(culamp_handle h, const double *x, const double *y, in
     auto body = [&](cudaStream_t cs) -> cudaError_t {
         cudaError_t e = launch_pass(pl.k1, pl.pm, ACC_LSE, pl.s_rows, S.scr, cs);
         if (e == cudaSuccess) e = launch_pass(pl.k2, pl.pm, ACC_LSE, pl.s_cols, S.scr, cs);
+        if (e == cudaSuccess) e = launch_pass(pl.k2m, pl.pm, ACC_LSE, pl.s_cols_mom, S.scr, cs);
         if (e == cudaSuccess)
-            e = launch_pass(pl.kd, pl.pm, pl.dual_min ? ACC_MIN : ACC_LSE, pl.s_rows, S.scr, cs);
+            e = launch_pass(pl.kd, pl.pm, pl.dual_min ? ACC_MIN : ACC_LSE,
+                            pl.dual_min ? pl.s_rows_min : pl.s_rows, S.scr, cs);
         if (e == cudaSuccess) e = launch_pass(pl.k3, pl.pm, ACC_LSE, pl.s_rows, S.scr, cs);
         if (e == cudaSuccess) e = launch_pass(pl.k4, pl.pm, ACC_LSE, pl.s_cols, S.scr, cs);
         return e;
@@ -731,8 +746,9 @@ extern "C" int culamp_lamp(culamp_handle h, const double *x, const double *y, in
         b.beta = a.beta;
         b.lamp_step = LAMP_NONE;
         b.want_moment = 1;
+        b.gate = GATE_ALWAYS;
         b.finish = FIN_SUMS;
-        CUDA_TRY(h, launch_pass(b, pl.pm, ACC_LSE, pl.s_cols, S.scr, st));
+        CUDA_TRY(h, launch_pass(b, pl.pm, ACC_LSE, pl.s_cols_mom, S.scr, st));
     }
     double sums[4];
     CUDA_TRY(h, cudaMemcpyAsync(sums, h->pass_ctl.as<Ctl>()->sums, sizeof(sums), cudaMemcpyDeviceToHost, st));
