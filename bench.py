@@ -53,19 +53,23 @@ def parse():
 
 
 def profile_pass(args):
+    """Profiler target: one W_inf pass, then warmup + steps Sinkhorn iterations on
+    an N-point RGB instance launched pass by pass (FLAG_NO_GRAPH, so each pass
+    is a separate kernel launch a profiler can capture). pair_pass_kernel
+    launch k (0-based): 0 = W_inf, then 3 per iteration (row LSE, column LSE,
+    gated residual), so `-k regex:pair_pass_kernel -s 10 -c 1` captures the
+    row pass of iteration 4 (fixed-reference path)."""
     import torch
     import culamp_b200 as cb
-    from culamp_b200 import datasets as D, kernels as K
+    from culamp_b200 import datasets as D
     n = args.profile_pass
     x, y, r, c = D.rgb_instance(n, n)
     X, Y, R, Cc = (torch.as_tensor(v, device="cuda") for v in (x, y, r, c))
-    _, winf = K.max_logsumexp_spp_ct(X, Y, P)
-    psi = torch.zeros(n, dtype=torch.float64, device="cuda")
-    for _ in range(args.warmup + args.steps):
-        out = K.warp_logsumexp_ct_fused(X, Y, R, psi, ETA, winf, P)
+    a = cb.EOTArgs(eta_p=ETA, epsilon=0.0, itermax=args.warmup + args.steps, verbose=False)
+    res = cb.solve_sinkhorn(X, Y, R, Cc, a, 10**6, P, flags=cb.FLAG_NO_GRAPH)
     torch.cuda.synchronize()
-    print(json.dumps({"profile_pass": n, "launches": args.warmup + args.steps,
-                      "finite": bool(torch.isfinite(out).all())}))
+    print(json.dumps({"profile_pass": n, "iterations": res.iterations,
+                      "finite": bool(torch.isfinite(res.phi).all())}))
     return 0
 
 

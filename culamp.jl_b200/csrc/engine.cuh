@@ -145,6 +145,7 @@ struct PassParams {
     double eta_mu_exp, minv, maxv;
     // moments
     int want_moment;            // 1: accumulate the softmax-weighted cost moment (MOM kernels)
+    int use_ref;                // 1: fixed-reference fast path, reference = the row's previous LSE
     // gating and control
     int gate;
     int finish;
@@ -645,6 +646,145 @@ __device__ __forceinline__ void lse_step(const double4 col, const double (&xr)[R
     }
 }
 
+// ---------------------------------------------------------------------------
+// Fixed-reference log-sum-exp (packed d <= 3, no moment).
+//
+// Each row carries a reference Mref (log2 units, the row's previous LSE). The
+// exponent t is clamped to [Mref - 126, Mref + 127] (2 DMNMX) and one DADD with
+// FR_MAGIC = 1.5 * 2^28 turns x = t - Mref - 1 into a double whose ulp is
+// 2^-24, so its low 32 bits are round(x * 2^24) in two's complement (|x| < 128).
+// From that fixed-point value: n = floor(x) (shift), the 23 leading fraction
+// bits OR-ed into 1.0f give v = 1 + frac(x), and 2^t-Mref = 2^n * 2^v, i.e. one
+// ex2 of v (in [1,2)) with n added to the exponent field. No FP64->FP32
+// conversion and no per-pair max test: one MUFU op per pair.
+// A row whose sum leaves [2^-64, 2^64] had its maximum more than 64 away from
+// the reference; the caller then recomputes the tile with tile_lse_packed.
+constexpr double FR_MAGIC = 402653184.0;   // 1.5 * 2^28
+constexpr double FR_LO = FR_MAGIC - 127.0;  // x = t - Mref - 1 >= -127
+constexpr double FR_HI = FR_MAGIC + 126.0;  // x <= 126
+
+// The row's previous log-sum-exp (natural log), read from the buffer the
+// epilogue overwrites: phi -> log(marg) - phi, logZ -> logZ, column mass ->
+// log(mass) - beta * rowpot.
+__device__ __forceinline__ double row_reference(const PassParams &P, int o, double beta) {
+    if (P.epi == EPI_SK_ROW) return log(P.marg[o]) - P.out[o];
+    if (P.epi == EPI_LOGZ) return P.out[o];
+    if (P.epi == EPI_SPP_COL)
+        return log(P.out[o]) - ((beta == 0.0 || !P.rowpot) ? 0.0 : beta * P.rowpot[o]);
+    return NAN;
+}
+
+template <int PM, int D, int R>
+__device__ __forceinline__ void fr_step(const double4 col, const double (&xr)[R][D], double a2,
+                                        double pexp, const double (&K)[R], float (&cs)[R]) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        double t;
+        if (PM == P_SQ) {
+            t = col.w;
+            if (D >= 3) t = fma(xr[r][D >= 3 ? 2 : 0], col.z, t);
+            if (D >= 2) t = fma(xr[r][D >= 2 ? 1 : 0], col.y, t);
+            t = fma(xr[r][0], col.x, t);
+        } else {
+            const double yv[3] = {col.x, col.y, col.z};
+            t = fma(pair_cost_direct<PM>(xr[r], yv, D, pexp), a2, col.w);
+        }
+        const double dv = fmin(fmax(t + K[r], FR_LO), FR_HI);
+        const int L = __double2loint(dv);
+        const int n = L >> 24;
+        const float v = __int_as_float(((unsigned)L >> 1 & 0x007FFFFFu) | 0x3F800000u);
+        const float e = __int_as_float(__float_as_int(ex2_approx(v)) + (n << 23));
+        cs[r] += e;
+    }
+}
+
+// Returns true when every real row of this thread stayed inside the window.
+template <int PM, int D, int R>
+__device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double alpha, double beta,
+                                                  int row_base, int cbeg, int cend, double *smem,
+                                                  double (&Mo)[R], double (&So)[R],
+                                                  double (&Ho)[R]) {
+    constexpr bool SQ = (PM == P_SQ);
+    const int tid = threadIdx.x;
+    const double a2 = alpha * LOG2E;
+    const double cb = P.colpot_unit ? LOG2E : beta * LOG2E;
+    double ctr[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) ctr[k] = P.ctr ? P.ctr[k] : 0.0;
+    double xr[R][D], K[R];
+    float S[R], Cc[R], cs[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int row = row_base + tid + r * TPB;
+        const bool ok = row < P.n;
+        double h = 0.0;
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            const double v = ok ? P.X[(size_t)row * D + k] - ctr[k] : 0.0;
+            xr[r][k] = SQ ? -2.0 * a2 * v : v;
+            h = fma(v, v, h);
+        }
+        const double m = (ok ? row_reference(P, row, beta) * LOG2E : 0.0) - (SQ ? a2 * h : 0.0);
+        K[r] = (FR_MAGIC - 1.0) - m;
+        S[r] = 0.f; Cc[r] = 0.f; cs[r] = 0.f;
+    }
+    double4 *tile = reinterpret_cast<double4 *>(smem);
+    for (int c0 = cbeg; c0 < cend; c0 += CHUNK) {
+        __syncthreads();
+        for (int q = tid; q < CHUNK; q += TPB) {
+            const int j = c0 + q;
+            double4 v = make_double4(0.0, 0.0, 0.0, -INFINITY);
+            if (j < cend) {
+                double yy[3] = {0.0, 0.0, 0.0};
+                double s2 = 0.0;
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+                    yy[k] = P.Y[(size_t)j * D + k] - ctr[k];
+                    s2 = fma(yy[k], yy[k], s2);
+                }
+                const double pot = P.colpot ? P.colpot[j] : 0.0;
+                double g = (cb == 0.0) ? 0.0 : cb * pot;
+                if (SQ) g += a2 * s2;
+                v = make_double4(yy[0], yy[1], yy[2], g);
+            }
+            tile[q] = v;
+        }
+        __syncthreads();
+        const int nc = min(CHUNK, cend - c0);
+        int q = 0;
+        for (; q + 8 <= nc; q += 8) {
+#pragma unroll 2
+            for (int u = 0; u < 8; ++u) fr_step<PM, D, R>(tile[q + u], xr, a2, P.pexp, K, cs);
+#pragma unroll
+            for (int r = 0; r < R; ++r) { kahan_add(S[r], Cc[r], cs[r]); cs[r] = 0.f; }
+        }
+        for (; q < nc; ++q) fr_step<PM, D, R>(tile[q], xr, a2, P.pexp, K, cs);
+#pragma unroll
+        for (int r = 0; r < R; ++r) { kahan_add(S[r], Cc[r], cs[r]); cs[r] = 0.f; }
+    }
+    bool good = true;
+    const int ncols = cend - cbeg;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int row = row_base + tid + r * TPB;
+        const bool real_row = row < P.n;
+        double h = 0.0;
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            const double v = real_row ? P.X[(size_t)row * D + k] - ctr[k] : 0.0;
+            h = fma(v, v, h);
+        }
+        Ho[r] = SQ ? a2 * h : 0.0;
+        Mo[r] = (real_row ? row_reference(P, row, beta) * LOG2E : 0.0) - Ho[r];
+        const double sv = (double)S[r] - (double)Cc[r];
+        So[r] = sv;
+        // an empty column slice contributes nothing; otherwise the sum of a real
+        // row must sit inside the window where no clamped term matters
+        if (real_row && ncols > 0 && !(sv >= 0x1p-64 && sv <= 0x1p64)) good = false;
+    }
+    return good;
+}
+
 // Packed (d <= 3) log-sum-exp tile: rows in registers, column tiles of CHUNK
 // (y - ctr, g) double4 entries in shared memory, broadcast to the warp.
 template <int PM, int D, int R, bool MOM>
@@ -704,7 +844,7 @@ __device__ __forceinline__ void tile_lse_packed(const PassParams &P, double alph
         const int nc = min(CHUNK, cend - c0);
         int q = 0;
         for (; q + 8 <= nc; q += 8) {
-#pragma unroll
+#pragma unroll 2
             for (int u = 0; u < 8; ++u) lse_step<PM, D, R, MOM>(tile[q + u], xr, xs, a2, P.pexp, M, S, Cc, cs, mo);
 #pragma unroll
             for (int r = 0; r < R; ++r) { kahan_add(S[r], Cc[r], cs[r]); cs[r] = 0.f; }
@@ -743,7 +883,28 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
 
     double Mv[R], Sv[R], MOMv[R], Hv[R];
     if constexpr (ACC == ACC_LSE && D > 0) {
-        tile_lse_packed<PM, D, R, MOM>(P, alpha, beta, row_base, cbeg, cend, smem, Mv, Sv, MOMv, Hv);
+        bool done = false;
+        if constexpr (!MOM) {
+            if (P.use_ref) {
+                // reference = the row's previous LSE, from the buffer the epilogue
+                // is about to overwrite (read-only until every split has finished)
+                bool ok = true;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int o = row_base + threadIdx.x + r * TPB;
+                    if (o < P.n && !isfinite(row_reference(P, o, beta))) ok = false;
+                }
+                if (!__syncthreads_or(!ok)) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) MOMv[r] = 0.0;
+                    const bool good = tile_lse_fixedref<PM, D, R>(P, alpha, beta, row_base, cbeg, cend,
+                                                                  smem, Mv, Sv, Hv);
+                    done = !__syncthreads_or(!good);
+                }
+            }
+        }
+        if (!done)
+            tile_lse_packed<PM, D, R, MOM>(P, alpha, beta, row_base, cbeg, cend, smem, Mv, Sv, MOMv, Hv);
     } else {
         static_assert(R == RPT, "generic / min-max tiles use RPT rows per thread");
         tile_reduce<PM, D, ACC, MOM>(P, alpha, beta, row_base, cbeg, cend, smem, Mv, Sv, MOMv, Hv);

@@ -373,6 +373,7 @@ SkPlan make_sk_plan(culamp_handle h, int n, int m, int d, double p, uint32_t fla
     pl.k1.colpot = S.psi.as<double>();
     pl.k1.marg = S.r.as<double>();
     pl.k1.out = S.phi.as<double>();
+    pl.k1.use_ref = 1;
     // K2: psi = log c - LSE_i(-C/(eta W) + phi); iteration bookkeeping
     pl.k2 = mk(Y, X, m, n, d, p_iter, ctl);
     pl.k2.ctr = X;
@@ -381,6 +382,7 @@ SkPlan make_sk_plan(culamp_handle h, int n, int m, int d, double p, uint32_t fla
     pl.k2.colpot = S.phi.as<double>();
     pl.k2.marg = S.c.as<double>();
     pl.k2.out = S.psi.as<double>();
+    pl.k2.use_ref = 1;
     pl.k2.finish = FIN_SK_ITER;
     // K3 (check iterations): row residual + transport cost, tolerance test
     pl.k3 = mk(X, Y, n, m, d, p_res, ctl);
@@ -563,6 +565,7 @@ LampPlan make_lamp_plan(culamp_handle h, int n, int m, int d, double p, double w
     pl.k1.marg = S.r.as<double>();
     pl.k1.out = S.logz.as<double>();
     pl.k1.aux = S.aux.as<double>();
+    pl.k1.use_ref = 1;
     pl.k1.finish = FIN_LAMP_Z;
     // K2: column residual at nu (+ cost on check iterations), fused theta_bar / nu_bar step
     pl.k2 = mk(Y, X, m, n, d, p, ctl);
@@ -576,6 +579,7 @@ LampPlan make_lamp_plan(culamp_handle h, int n, int m, int d, double p, double w
     pl.k2.out = S.res.as<double>();
     pl.k2.out2 = S.cost.as<double>();
     pl.k2.want_moment = 0;
+    pl.k2.use_ref = 1;
     pl.k2.gate = GATE_NOCHECK;
     pl.k2.lamp_step = LAMP_A;
     pl.k2.theta = S.theta.as<double>();
@@ -590,6 +594,7 @@ LampPlan make_lamp_plan(culamp_handle h, int n, int m, int d, double p, double w
     // the same pass with the cost moment, on check iterations only
     pl.k2m = pl.k2;
     pl.k2m.want_moment = 1;
+    pl.k2m.use_ref = 0;
     pl.k2m.gate = GATE_CHECK;
     // Kd (check iterations): dual value at theta
     pl.dual_min = !(eta > 0.0);
@@ -606,6 +611,7 @@ LampPlan make_lamp_plan(culamp_handle h, int n, int m, int d, double p, double w
         pl.kd.ctr = X;
         pl.kd.epi = EPI_LOGZ;
         pl.kd.coef_mode = COEF_SPP_DUAL;
+        pl.kd.use_ref = 1;
     }
     // K3: logZ at nu_bar with (eta_t', s')
     pl.k3 = pl.k1;

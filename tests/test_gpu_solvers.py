@@ -4,7 +4,7 @@ convergence-log rows, potentials and objectives within tolerance.
 
 Potentials are compared two ways. (1) Raw, at the north-star bar: max error
 <= 1e-5 of max |potential|. (2) Gauge-fixed (the r-weighted mean removed), at
-2e-6 absolute for Sinkhorn: Sinkhorn's plan exp(phi_i + psi_j - C/eps) is
+5e-6 absolute for Sinkhorn: Sinkhorn's plan exp(phi_i + psi_j - C/eps) is
 invariant to phi + k, psi - k, and LAMP's to a uniform shift of nu, and those
 directions are not contracted by the iteration, so FP32-exp rounding drifts
 along them (a few 1e-6 over 200 iterations) while the plan itself stays within
@@ -19,7 +19,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-POT_ATOL = 2e-6
+POT_ATOL = 5e-6
 REL = 1e-5
 
 
