@@ -649,19 +649,24 @@ __device__ __forceinline__ void lse_step(const double4 col, const double (&xr)[R
 // ---------------------------------------------------------------------------
 // Fixed-reference log-sum-exp (packed d <= 3, no moment).
 //
-// Each row carries a reference Mref (log2 units, the row's previous LSE). The
-// exponent t is clamped to [Mref - 126, Mref + 127] (2 DMNMX) and one DADD with
-// FR_MAGIC = 1.5 * 2^28 turns x = t - Mref - 1 into a double whose ulp is
-// 2^-24, so its low 32 bits are round(x * 2^24) in two's complement (|x| < 128).
-// From that fixed-point value: n = floor(x) (shift), the 23 leading fraction
-// bits OR-ed into 1.0f give v = 1 + frac(x), and 2^t-Mref = 2^n * 2^v, i.e. one
-// ex2 of v (in [1,2)) with n added to the exponent field. No FP64->FP32
-// conversion and no per-pair max test: one MUFU op per pair.
-// A row whose sum leaves [2^-64, 2^64] had its maximum more than 64 away from
-// the reference; the caller then recomputes the tile with tile_lse_packed.
-constexpr double FR_MAGIC = 402653184.0;   // 1.5 * 2^28
-constexpr double FR_LO = FR_MAGIC - 127.0;  // x = t - Mref - 1 >= -127
-constexpr double FR_HI = FR_MAGIC + 126.0;  // x <= 126
+// Each row carries a reference Mref (log2 units, the row's previous LSE). With
+// x = t - Mref - 1, one DADD forms D = x + 1.5*2^20 (+2^-24 so the truncation
+// below rounds). D's ulp is 2^-32, so for |x| < 2^19 its high word carries
+// 2^19 + floor(x) in its low 20 bits and its low word is frac(x) * 2^32. Then
+//   * n = floor(x) is clamped to [-127, 126] by two 32-bit integer min/max on
+//     the high word (IEEE bit patterns are monotone in the value, so +-inf and
+//     out-of-range x clamp correctly);
+//   * a funnel shift of the low word under 0x7F gives v = 1 + frac(x) (23 bits);
+//   * 2^(t - Mref) = 2^(1 + x) = ex2(v) * 2^n: one MUFU ex2, and n is added to the
+//     exponent field as (hi << 23) (the 2^19 offset vanishes modulo 2^32).
+// No FP64->FP32 conversion, no FP64 min/max, no per-pair max test.
+// Clamped-low terms contribute < 2^-125 each; a row whose sum leaves
+// [2^-64, 2^64] (reference more than ~64 from the true LSE, or a term clamped
+// high, or a non-finite input) makes the CTA recompute with tile_lse_packed.
+constexpr double FR_MAGIC = 1572864.0 + 0x1p-24;   // 1.5 * 2^20, plus the rounding half-ulp
+constexpr int FR_H0 = 0x41380000;                  // high word of 1.5 * 2^20 (n = 0)
+constexpr int FR_HLO = FR_H0 - 127;
+constexpr int FR_HHI = FR_H0 + 126;
 
 // The row's previous log-sum-exp (natural log), read from the buffer the
 // epilogue overwrites: phi -> log(marg) - phi, logZ -> logZ, column mass ->
@@ -689,11 +694,10 @@ __device__ __forceinline__ void fr_step(const double4 col, const double (&xr)[R]
             const double yv[3] = {col.x, col.y, col.z};
             t = fma(pair_cost_direct<PM>(xr[r], yv, D, pexp), a2, col.w);
         }
-        const double dv = fmin(fmax(t + K[r], FR_LO), FR_HI);
-        const int L = __double2loint(dv);
-        const int n = L >> 24;
-        const float v = __int_as_float(((unsigned)L >> 1 & 0x007FFFFFu) | 0x3F800000u);
-        const float e = __int_as_float(__float_as_int(ex2_approx(v)) + (n << 23));
+        const double dv = t + K[r];
+        const int hi = min(max(__double2hiint(dv), FR_HLO), FR_HHI);
+        const float v = __int_as_float((int)__funnelshift_r((unsigned)__double2loint(dv), 0x7Fu, 9));
+        const float e = __int_as_float(__float_as_int(ex2_approx(v)) + (hi << 23));
         cs[r] += e;
     }
 }
@@ -725,7 +729,7 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
             h = fma(v, v, h);
         }
         const double m = (ok ? row_reference(P, row, beta) * LOG2E : 0.0) - (SQ ? a2 * h : 0.0);
-        K[r] = (FR_MAGIC - 1.0) - m;
+        K[r] = FR_MAGIC - (m + 1.0);
         S[r] = 0.f; Cc[r] = 0.f; cs[r] = 0.f;
     }
     double4 *tile = reinterpret_cast<double4 *>(smem);
