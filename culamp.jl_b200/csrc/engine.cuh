@@ -660,9 +660,13 @@ __device__ __forceinline__ void lse_step(const double4 col, const double (&xr)[R
 //   * 2^(t - Mref) = 2^(1 + x) = ex2(v) * 2^n: one MUFU ex2, and n is added to the
 //     exponent field as (hi << 23) (the 2^19 offset vanishes modulo 2^32).
 // No FP64->FP32 conversion, no FP64 min/max, no per-pair max test.
-// Clamped-low terms contribute < 2^-125 each; a row whose sum leaves
-// [2^-64, 2^64] (reference more than ~64 from the true LSE, or a term clamped
-// high, or a non-finite input) makes the CTA recompute with tile_lse_packed.
+// Clamped-low terms contribute < 2^-125 each. A column slice whose partial sum
+// exceeds 2^64 (a term clamped high, or a non-finite input) is recomputed by its
+// CTA with tile_lse_packed; after the slices are merged, a row whose full LSE
+// lies more than 61 (log2 units) below its reference -- where the clamped-low
+// terms could matter -- makes the merging CTA recompute its row block over all
+// columns the same way.
+constexpr double FR_LOW_MARGIN = 61.0;
 constexpr double FR_MAGIC = 1572864.0 + 0x1p-24;   // 1.5 * 2^20, plus the rounding half-ulp
 constexpr int FR_H0 = 0x41380000;                  // high word of 1.5 * 2^20 (n = 0)
 constexpr int FR_HLO = FR_H0 - 127;
@@ -702,7 +706,8 @@ __device__ __forceinline__ void fr_step(const double4 col, const double (&xr)[R]
     }
 }
 
-// Returns true when every real row of this thread stayed inside the window.
+// Returns false when a real row's partial sum overflowed the window (a term
+// clamped high, or a non-finite input).
 template <int PM, int D, int R>
 __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double alpha, double beta,
                                                   int row_base, int cbeg, int cend, double *smem,
@@ -767,7 +772,6 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
         for (int r = 0; r < R; ++r) { kahan_add(S[r], Cc[r], cs[r]); cs[r] = 0.f; }
     }
     bool good = true;
-    const int ncols = cend - cbeg;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int row = row_base + tid + r * TPB;
@@ -782,9 +786,9 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
         Mo[r] = (real_row ? row_reference(P, row, beta) * LOG2E : 0.0) - Ho[r];
         const double sv = (double)S[r] - (double)Cc[r];
         So[r] = sv;
-        // an empty column slice contributes nothing; otherwise the sum of a real
-        // row must sit inside the window where no clamped term matters
-        if (real_row && ncols > 0 && !(sv >= 0x1p-64 && sv <= 0x1p64)) good = false;
+        // this slice's partial sum must not hold a term clamped high; a small
+        // partial is fine (the lower side is checked on the merged row)
+        if (real_row && !(sv <= 0x1p64)) good = false;
     }
     return good;
 }
@@ -886,6 +890,7 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
     const int cend = min(P.m, cbeg + P.cols_per_split);
 
     double Mv[R], Sv[R], MOMv[R], Hv[R];
+    bool fr_tried = false;   // the fixed-reference path ran for this row block
     if constexpr (ACC == ACC_LSE && D > 0) {
         bool done = false;
         if constexpr (!MOM) {
@@ -899,6 +904,7 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
                     if (o < P.n && !isfinite(row_reference(P, o, beta))) ok = false;
                 }
                 if (!__syncthreads_or(!ok)) {
+                    fr_tried = true;
 #pragma unroll
                     for (int r = 0; r < R; ++r) MOMv[r] = 0.0;
                     const bool good = tile_lse_fixedref<PM, D, R>(P, alpha, beta, row_base, cbeg, cend,
@@ -948,6 +954,26 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
             Mv[r] = M; Sv[r] = S; MOMv[r] = MO;
         }
         if (threadIdx.x == 0) P.rb_ticket[rb] = 0u;   // re-arm for the next launch
+    }
+
+    if constexpr (ACC == ACC_LSE && D > 0 && !MOM) {
+        // Lower side of the fixed-reference window, on the merged row: the full
+        // LSE must be within FR_LOW_MARGIN of the reference, else clamped-low
+        // terms could matter and the row block is recomputed over all columns.
+        if (fr_tried) {
+            const double a2 = alpha * LOG2E;
+            bool bad = false;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int o = row_base + threadIdx.x + r * TPB;
+                if (o >= P.n) continue;
+                const double mref = row_reference(P, o, beta) * LOG2E - Hv[r];
+                if (!(Sv[r] > 0.0) || Mv[r] + log2(Sv[r]) < mref - FR_LOW_MARGIN) bad = true;
+            }
+            (void)a2;
+            if (__syncthreads_or(bad))
+                tile_lse_packed<PM, D, R, false>(P, alpha, beta, row_base, 0, P.m, smem, Mv, Sv, MOMv, Hv);
+        }
     }
 
     // ---------------- epilogue: one thread per output row
