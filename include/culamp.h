@@ -207,6 +207,22 @@ int culamp_marginal_error_fp64(culamp_handle h, const double *x, const double *y
                                const double *phi, const double *psi, double reg, double winf,
                                double p, double *row_l1, double *col_l1, void *stream);
 
+/* Scratch-free variant of culamp_lse_rows_sk, for callers that cannot let the
+ * library allocate device memory when they call it: code recording a CUDA stream
+ * capture (cudaMalloc cannot be captured) and hosts that own all device memory
+ * through their own pool or budget. No counterpart in the reference (its kernels
+ * allocate nothing, but its solvers allocate their caches with CuArray).
+ * Same arguments and result as culamp_lse_rows_sk, without a handle. Its scratch
+ * is fixed file-scope device memory (3 MiB of split partials + 256 KiB of
+ * tickets, held on every GPU that loads the library until exit); n is limited
+ * to 16,777,216 rows (CULAMP_ERR_UNSUPPORTED beyond). The first call on a device
+ * resolves that memory's address and may load the module: make it before any
+ * stream capture. All calls share the scratch, so calls that overlap on the GPU
+ * race; serialise them. Calls no cudaMalloc / cudaFree. */
+int culamp_lse_rows_sk_noalloc(double *out, const double *x, const double *y, int64_t n,
+                               int64_t m, int32_t d, const double *marg, const double *pot,
+                               double reg, double winf, double p, void *stream);
+
 /* ------------------------------------------------------------ diagnostics
  * No counterpart in the reference. Measures, on the running GPU, the sustained
  * instruction rates that bound the pair passes: out[0] = DFMA/s, out[1] = MUFU
