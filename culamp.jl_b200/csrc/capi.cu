@@ -293,6 +293,7 @@ extern "C" int culamp_lse_rows_sk(culamp_handle h, double *out, const double *x,
     P.colpot = pot;
     P.marg = marg;
     P.out = out;
+    P.use_ref = 1;   // out's previous content (the last phi) is the reference hint
     return run_pass(h, P, pmode_of(p), ACC_LSE, (cudaStream_t)stream);
 }
 
@@ -331,6 +332,7 @@ extern "C" int culamp_lse_rows_spp(culamp_handle h, double *out, const double *x
     P.beta = -invreg;
     P.colpot = theta;
     P.out = out;
+    P.use_ref = 1;   // out's previous content (the last logZ) is the reference hint
     return run_pass(h, P, pmode_of(p), ACC_LSE, (cudaStream_t)stream);
 }
 

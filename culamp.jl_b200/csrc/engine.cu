@@ -43,9 +43,9 @@ LaunchShape pass_shape(int n, int m, int d, int acc, int sm_count, bool mom) {
     return s;
 }
 
-template <int PM, int D, int ACC, int R, bool MOM>
+template <int PM, int D, int ACC, int R, bool MOM, bool FR = false>
 static cudaError_t launch_t(const PassParams &P, const LaunchShape &sh, cudaStream_t st) {
-    auto kern = pair_pass_kernel<PM, D, ACC, R, MOM>;
+    auto kern = pair_pass_kernel<PM, D, ACC, R, MOM, FR>;
     if (sh.smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)sh.smem);
@@ -60,8 +60,13 @@ template <int PM, int D, int ACC>
 static cudaError_t launch_v(const PassParams &P, const LaunchShape &sh, cudaStream_t st) {
     if constexpr (ACC == ACC_LSE) {
         if (P.want_moment) return launch_t<PM, D, ACC, RPT, true>(P, sh, st);
-        if constexpr (D > 0)
+        if constexpr (D > 0) {
+            if (P.use_ref) {
+                if (sh.R == RPT_BIG) return launch_t<PM, D, ACC, RPT_BIG, false, true>(P, sh, st);
+                return launch_t<PM, D, ACC, RPT, false, true>(P, sh, st);
+            }
             if (sh.R == RPT_BIG) return launch_t<PM, D, ACC, RPT_BIG, false>(P, sh, st);
+        }
     }
     return launch_t<PM, D, ACC, RPT, false>(P, sh, st);
 }

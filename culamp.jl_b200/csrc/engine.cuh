@@ -795,7 +795,7 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
 
 // Packed (d <= 3) log-sum-exp tile: rows in registers, column tiles of CHUNK
 // (y - ctr, g) double4 entries in shared memory, broadcast to the warp.
-template <int PM, int D, int R, bool MOM>
+template <int PM, int D, int R, bool MOM, int UNROLL = 8>
 __device__ __forceinline__ void tile_lse_packed(const PassParams &P, double alpha, double beta,
                                                 int row_base, int cbeg, int cend, double *smem,
                                                 double (&Mo)[R], double (&So)[R],
@@ -852,7 +852,7 @@ __device__ __forceinline__ void tile_lse_packed(const PassParams &P, double alph
         const int nc = min(CHUNK, cend - c0);
         int q = 0;
         for (; q + 8 <= nc; q += 8) {
-#pragma unroll 2
+#pragma unroll UNROLL
             for (int u = 0; u < 8; ++u) lse_step<PM, D, R, MOM>(tile[q + u], xr, xs, a2, P.pexp, M, S, Cc, cs, mo);
 #pragma unroll
             for (int r = 0; r < R; ++r) { kahan_add(S[r], Cc[r], cs[r]); cs[r] = 0.f; }
@@ -869,7 +869,10 @@ __device__ __forceinline__ void tile_lse_packed(const PassParams &P, double alph
     }
 }
 
-template <int PM, int D, int ACC, int R, bool MOM>
+// FR: this instantiation tries the fixed-reference loop first (P.use_ref must be
+// set) and carries a compact online loop for its fallbacks; FR == false runs
+// the online loop alone, fully unrolled.
+template <int PM, int D, int ACC, int R, bool MOM, bool FR>
 __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassParams P) {
     extern __shared__ __align__(16) double smem[];
     __shared__ double red[4 * (TPB / 32)];
@@ -893,8 +896,8 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
     bool fr_tried = false;   // the fixed-reference path ran for this row block
     if constexpr (ACC == ACC_LSE && D > 0) {
         bool done = false;
-        if constexpr (!MOM) {
-            if (P.use_ref) {
+        if constexpr (FR && !MOM) {
+            {
                 // reference = the row's previous LSE, from the buffer the epilogue
                 // is about to overwrite (read-only until every split has finished)
                 bool ok = true;
@@ -913,8 +916,10 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
                 }
             }
         }
-        if (!done)
-            tile_lse_packed<PM, D, R, MOM>(P, alpha, beta, row_base, cbeg, cend, smem, Mv, Sv, MOMv, Hv);
+        if (!done) {
+            if constexpr (FR) tile_lse_packed<PM, D, R, MOM, 2>(P, alpha, beta, row_base, cbeg, cend, smem, Mv, Sv, MOMv, Hv);
+            else tile_lse_packed<PM, D, R, MOM, 8>(P, alpha, beta, row_base, cbeg, cend, smem, Mv, Sv, MOMv, Hv);
+        }
     } else {
         static_assert(R == RPT, "generic / min-max tiles use RPT rows per thread");
         tile_reduce<PM, D, ACC, MOM>(P, alpha, beta, row_base, cbeg, cend, smem, Mv, Sv, MOMv, Hv);
@@ -956,7 +961,7 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
         if (threadIdx.x == 0) P.rb_ticket[rb] = 0u;   // re-arm for the next launch
     }
 
-    if constexpr (ACC == ACC_LSE && D > 0 && !MOM) {
+    if constexpr (FR && ACC == ACC_LSE && D > 0 && !MOM) {
         // Lower side of the fixed-reference window, on the merged row: the full
         // LSE must be within FR_LOW_MARGIN of the reference, else clamped-low
         // terms could matter and the row block is recomputed over all columns.
@@ -972,7 +977,7 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
             }
             (void)a2;
             if (__syncthreads_or(bad))
-                tile_lse_packed<PM, D, R, false>(P, alpha, beta, row_base, 0, P.m, smem, Mv, Sv, MOMv, Hv);
+                tile_lse_packed<PM, D, R, false, 2>(P, alpha, beta, row_base, 0, P.m, smem, Mv, Sv, MOMv, Hv);
         }
     }
 

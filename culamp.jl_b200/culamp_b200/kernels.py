@@ -35,11 +35,13 @@ def max_logsumexp_spp_ct(x, y, p):
     return out, w.value
 
 
-def warp_logsumexp_ct_fused(x, y, marginal, pot, reg, winf, p):
-    """SinkhornKernel.jl:341-444: log(marg_i) - LSE_j(-C_ij/(reg W) + pot_j)."""
+def warp_logsumexp_ct_fused(x, y, marginal, pot, reg, winf, p, out=None):
+    """SinkhornKernel.jl:341-444: log(marg_i) - LSE_j(-C_ij/(reg W) + pot_j).
+    With `out` given the result overwrites it in place, and its previous
+    content (the last phi of an iteration) serves as the kernel's reference."""
     n, d = x.shape
     m = y.shape[0]
-    out = _empty(n, x)
+    out = _empty(n, x) if out is None else out
     h = _h(x)
     h.check(h._lib.culamp_lse_rows_sk(h.ptr, C.c_void_p(out.data_ptr()), _dev(x, "x"),
                                       _dev(y, "y"), n, m, d, _dev(marginal, "marginal", n),
@@ -62,11 +64,12 @@ def residual_opt(x, y, marginal, phi, psi, reg, winf, p):
     return res, cost
 
 
-def warp_logsumexp_spp_ct_fused(x, y, theta, reg, st, winf, p):
-    """MirrorProxKernel.jl:833-938: LSE_j(-(C_ij st/(2W) + theta_j)/reg)."""
+def warp_logsumexp_spp_ct_fused(x, y, theta, reg, st, winf, p, out=None):
+    """MirrorProxKernel.jl:833-938: LSE_j(-(C_ij st/(2W) + theta_j)/reg); `out`
+    as for warp_logsumexp_ct_fused."""
     n, d = x.shape
     m = y.shape[0]
-    out = _empty(n, x)
+    out = _empty(n, x) if out is None else out
     h = _h(x)
     h.check(h._lib.culamp_lse_rows_spp(h.ptr, C.c_void_p(out.data_ptr()), _dev(x, "x"),
                                        _dev(y, "y"), n, m, d, _dev(theta, "theta", m), float(reg),

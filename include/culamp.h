@@ -109,7 +109,11 @@ int culamp_max_cost(culamp_handle h, const double *x, const double *y, int64_t n
                     int32_t d, double p, double *rowmax, double *winf_host, void *stream);
 
 /* warp_logsumexp_ct_fused! (SinkhornKernel.jl:341-444):
- * out[i] = log(marg[i]) - LSE_j(-C(x_i,y_j)/(reg*winf) + pot[j]). */
+ * out[i] = log(marg[i]) - LSE_j(-C(x_i,y_j)/(reg*winf) + pot[j]).
+ * out is overwritten in place, as the reference updates phi; its previous
+ * content (e.g. the last iteration's phi) is read as a hint that enables the
+ * fixed-reference fast path. Any previous content is valid: a missing, stale or
+ * non-finite hint only makes the kernel fall back to its online loop. */
 int culamp_lse_rows_sk(culamp_handle h, double *out, const double *x, const double *y,
                        int64_t n, int64_t m, int32_t d, const double *marg, const double *pot,
                        double reg, double winf, double p, void *stream);
@@ -124,7 +128,8 @@ int culamp_residual_sk(culamp_handle h, double *res, double *cost, const double 
                        void *stream);
 
 /* warp_logsumexp_spp_ct_fused! (MirrorProxKernel.jl:833-938):
- * out[i] = LSE_j(-(C_ij * st/(2 winf) + theta[j]) / reg). reg = +Inf is allowed. */
+ * out[i] = LSE_j(-(C_ij * st/(2 winf) + theta[j]) / reg). reg = +Inf is allowed.
+ * out's previous content (the last logZ) is a hint, as for culamp_lse_rows_sk. */
 int culamp_lse_rows_spp(culamp_handle h, double *out, const double *x, const double *y,
                         int64_t n, int64_t m, int32_t d, const double *theta, double reg,
                         double st, double winf, double p, void *stream);
