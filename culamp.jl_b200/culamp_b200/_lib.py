@@ -97,6 +97,8 @@ SIGNATURES = {
                                    _D, _U32, _VP, _VP, _VP, _VP, C.POINTER(CStats),
                                    C.POINTER(CLogRow), _I64]),
     "culamp_probe_pipes": (C.c_int, [_VP, C.POINTER(_D), _VP]),
+    "culamp_adjoint_sk": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, _D, _D, _D,
+                                    _VP]),
     "culamp_lse_rows_sk_noalloc": (C.c_int, [_VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, _D, _D, _D,
                                              _VP]),
     "culamp_marginal_error_fp64": (C.c_int, [_VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, _VP, _VP,

@@ -160,6 +160,16 @@ int culamp_barycentric_sk(culamp_handle h, double *out, const double *x, const d
                           int64_t n, int64_t m, int32_t d, const double *phi, const double *psi,
                           double reg, double winf, double p, void *stream);
 
+/* Adjoint of the Sinkhorn transport cost. No direct counterpart in the
+ * reference; it has the row-reduction shape of naive_findmaxindex_ct!
+ * (SinkhornKernel.jl:124-162). With P_ij = exp(phi[i] + psi[j] - C_ij/(reg*winf)):
+ *   grad[i*d+k] = sum_j P_ij dC(x_i, y_j)/dx_ik,   mass[i] = sum_j P_ij (may be NULL).
+ * At optimal potentials grad is d OT_eps / d x_i (envelope theorem, eps = reg*winf
+ * held fixed), computed without storing the n x m plan. 1 <= d <= 4. */
+int culamp_adjoint_sk(culamp_handle h, double *grad, double *mass, const double *x,
+                      const double *y, int64_t n, int64_t m, int32_t d, const double *phi,
+                      const double *psi, double reg, double winf, double p, void *stream);
+
 /* --------------------------------------------------------- solver level
  * Device pointers; the call returns when the solve has finished (it reads the
  * convergence state back once per batch of graph-launched iterations).

@@ -232,6 +232,45 @@ void or_barycentric_sk(double *out, const double *x, const double *y, int64_t n,
     }
 }
 
+/* Envelope gradient sum_j P_ij grad_x C(x_i, y_j), all FP64 (the cost
+ * derivative of the reference's costs: p=2 -> 2 d, p=1 -> sign d, p=Inf ->
+ * sign d on the first maximising coordinate, other p -> p |d|^(p-1) sign d). */
+void or_envelope_grad(double *grad, double *mass, const double *x, const double *y, int64_t n,
+                      int64_t m, int d, const double *phi, const double *psi, double reg,
+                      double winf, double p, const int64_t *rows, int64_t nrows) {
+    if (!rows) nrows = n;
+    const double k = -1.0 / (reg * winf);
+#pragma omp parallel for schedule(static)
+    for (int64_t q = 0; q < nrows; ++q) {
+        const int64_t i = rows ? rows[q] : q;
+        double g[64] = {0};
+        double s = 0.0;
+        for (int64_t j = 0; j < m; ++j) {
+            const double *xi = x + i * d, *yj = y + j * d;
+            const double pij = exp(or_cost(xi, yj, d, p) * k + phi[i] + psi[j]);
+            s += pij;
+            int kmax = 0;
+            double vmax = -1.0;
+            for (int kk = 0; kk < d; ++kk) {
+                double a = fabs(xi[kk] - yj[kk]);
+                if (a > vmax) { vmax = a; kmax = kk; }
+            }
+            for (int kk = 0; kk < d && kk < 64; ++kk) {
+                const double df = xi[kk] - yj[kk];
+                const double sg = (df > 0) - (df < 0);
+                double dc;
+                if (p == 2.0) dc = 2.0 * df;
+                else if (p == 1.0) dc = sg;
+                else if (isinf(p)) dc = (kk == kmax) ? sg : 0.0;
+                else dc = fabs(df) > 0 ? p * pow(fabs(df), p - 1.0) * sg : 0.0;
+                g[kk] += pij * dc;
+            }
+        }
+        for (int kk = 0; kk < d && kk < 64; ++kk) grad[q * d + kk] = g[kk];
+        if (mass) mass[q] = s;
+    }
+}
+
 static double l1_norm(const double *v, int64_t n) {
     double s = 0.0;
     for (int64_t i = 0; i < n; ++i) s += fabs(v[i]);

@@ -83,6 +83,14 @@ void or_barycentric_sk(double *out, const double *x, const double *y, int64_t n,
                        int d, const double *phi, const double *psi, double reg, double winf,
                        double cost_p);
 
+/* FP64 envelope gradient of the Sinkhorn transport cost (checker for the
+ * adjoint pass): grad[i*d+k] = sum_j P_ij dC/dx_ik, mass[i] = sum_j P_ij,
+ * P_ij = exp(phi_i + psi_j - C_ij/(reg W_inf)). Rows listed in `rows` (count
+ * nrows) only; rows == NULL means all n. Output rows are compact (nrows x d). */
+void or_envelope_grad(double *grad, double *mass, const double *x, const double *y, int64_t n,
+                      int64_t m, int d, const double *phi, const double *psi, double reg,
+                      double winf, double p, const int64_t *rows, int64_t nrows);
+
 /* Solver drivers. phi0/psi0 may be NULL. log may be NULL. */
 int or_sinkhorn_kernel(const double *x, const double *y, int64_t n, int64_t m, int d,
                        const double *r, const double *c, const or_args *args, int64_t frequency,

@@ -206,6 +206,22 @@ def barycentric_sk(x, y, phi, psi, reg, winf, cost_p):
     return out
 
 
+def envelope_grad(x, y, phi, psi, reg, winf, p, rows=None):
+    """FP64 sum_j P_ij grad_x C(x_i, y_j) and sum_j P_ij for the listed rows."""
+    x, y, phi, psi = map(_c64, (x, y, phi, psi))
+    d = x.shape[1]
+    ridx = None if rows is None else np.ascontiguousarray(rows, dtype=np.int64)
+    k = x.shape[0] if ridx is None else ridx.shape[0]
+    grad = np.empty((k, d))
+    mass = np.empty(k)
+    lib().or_envelope_grad(_p(grad), _p(mass), _p(x), _p(y), C.c_int64(x.shape[0]),
+                           C.c_int64(y.shape[0]), C.c_int(d), _p(phi), _p(psi), C.c_double(reg),
+                           C.c_double(winf), C.c_double(p),
+                           ridx.ctypes.data_as(C.POINTER(C.c_int64)) if ridx is not None else None,
+                           C.c_int64(k))
+    return grad, mass
+
+
 def sinkhorn_kernel(x, y, r, c, args: Args, frequency=100, p=2.0, phi0=None, psi0=None,
                     flags=0, log_cap=100000):
     x, y, r, c = map(_c64, (x, y, r, c))
