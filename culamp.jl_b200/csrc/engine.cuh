@@ -761,8 +761,11 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
         __syncthreads();
         const int nc = min(CHUNK, cend - c0);
         int q = 0;
+        // few rows per thread (small problems): unroll more columns so each warp
+        // has enough independent pairs in flight to cover FP64 / MUFU latency
+        constexpr int FR_UNROLL = (R > RPT) ? 2 : 8;
         for (; q + 8 <= nc; q += 8) {
-#pragma unroll 2
+#pragma unroll FR_UNROLL
             for (int u = 0; u < 8; ++u) fr_step<PM, D, R>(tile[q + u], xr, a2, P.pexp, K, cs);
 #pragma unroll
             for (int r = 0; r < R; ++r) { kahan_add(S[r], Cc[r], cs[r]); cs[r] = 0.f; }
@@ -949,12 +952,26 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
             const int row = row_base + threadIdx.x + r * TPB;
             if (row >= P.n) continue;
             double M = (ACC == ACC_MIN) ? INFINITY : -INFINITY, S = 0.0, MO = 0.0;
-            for (int s2 = 0; s2 < P.splits; ++s2) {
-                const volatile double *pp = P.part + ((size_t)s2 * P.n + row) * 3;
-                const double m2 = pp[0], ss2 = pp[1], mo2 = pp[2];
-                if (ACC == ACC_LSE) merge_lse(M, S, MO, m2, ss2, mo2);
-                else if (ACC == ACC_MAX) M = fmax(M, m2);
-                else M = fmin(M, m2);
+            // partials come from other CTAs: L2-coherent loads, issued 8 splits at a
+            // time so their latencies overlap, then merged in split order
+            for (int s0 = 0; s0 < P.splits; s0 += 8) {
+                double m2[8], ss2[8], mo2[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (s0 + u < P.splits) {
+                        const double *pp = P.part + ((size_t)(s0 + u) * P.n + row) * 3;
+                        m2[u] = __ldcg(pp);
+                        ss2[u] = __ldcg(pp + 1);
+                        mo2[u] = __ldcg(pp + 2);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (s0 + u >= P.splits) break;
+                    if (ACC == ACC_LSE) merge_lse(M, S, MO, m2[u], ss2[u], mo2[u]);
+                    else if (ACC == ACC_MAX) M = fmax(M, m2[u]);
+                    else M = fmin(M, m2[u]);
+                }
             }
             Mv[r] = M; Sv[r] = S; MOMv[r] = MO;
         }
