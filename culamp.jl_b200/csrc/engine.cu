@@ -23,6 +23,9 @@ LaunchShape pass_shape(int n, int m, int d, int acc, int sm_count, bool mom) {
     const int rows = TPB * s.R;
     s.rb = (n + rows - 1) / rows;
     if (s.rb < 1) s.rb = 1;
+    // column splits are whole tiles: measured at n = m = 4096, finer splits
+    // (64 / 128 columns) cost more in per-CTA overhead and merging than the
+    // extra CTAs win back
     const int ch = packed ? CHUNK : CHUNK_G;
     // Aim for ~4 resident CTAs per SM over the whole grid; never split below one tile.
     const int target = 4 * (sm_count > 0 ? sm_count : 148);

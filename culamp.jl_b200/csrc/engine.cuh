@@ -424,6 +424,11 @@ __device__ __forceinline__ void merge_lse(double &M, double &S, double &MOM, dou
                                           double MOM2) {
     if (M2 == -INFINITY || S2 == 0.0) return;
     if (M == -INFINITY || S == 0.0) { M = M2; S = S2; MOM = MOM2; return; }
+    if (M2 == M) {   // fixed-reference partials share one max: exp2(0) = 1 exactly
+        S += S2;
+        MOM += MOM2;
+        return;
+    }
     if (M2 > M) {
         const double f = exp2(M - M2);
         S = S * f + S2;
@@ -935,7 +940,8 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
             const int row = row_base + threadIdx.x + r * TPB;
             if (row < P.n) {
                 double *pp = P.part + ((size_t)sp * P.n + row) * 3;
-                pp[0] = Mv[r]; pp[1] = Sv[r]; pp[2] = MOMv[r];
+                pp[0] = Mv[r]; pp[1] = Sv[r];
+                if (MOM) pp[2] = MOMv[r];
             }
         }
         __threadfence();
@@ -962,7 +968,7 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
                         const double *pp = P.part + ((size_t)(s0 + u) * P.n + row) * 3;
                         m2[u] = __ldcg(pp);
                         ss2[u] = __ldcg(pp + 1);
-                        mo2[u] = __ldcg(pp + 2);
+                        mo2[u] = MOM ? __ldcg(pp + 2) : 0.0;
                     }
                 }
 #pragma unroll
