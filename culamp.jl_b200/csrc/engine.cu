@@ -42,6 +42,7 @@ LaunchShape pass_shape(int n, int m, int d, int acc, int sm_count, bool mom) {
     s.cols_per_split = cps;
     s.smem = (size_t)(packed ? CHUNK * 4 : CHUNK_G * (d + 1)) * sizeof(double);
     s.part_bytes = splits > 1 ? (size_t)splits * (size_t)n * 3 * sizeof(double) : 0;
+    s.sms = sm_count > 0 ? sm_count : 148;
     (void)acc;
     return s;
 }
@@ -96,6 +97,7 @@ static cudaError_t launch_p(const PassParams &P, int pm, const LaunchShape &sh, 
 
 cudaError_t launch_pass(PassParams P, int pm, int acc, const LaunchShape &sh, Scratch &scr,
                         cudaStream_t st) {
+    if (P.fx) return launch_feat_pass(P, acc, scr, sh.sms, st);       // tensor-core feature path
     if (P.want_moment && sh.R != RPT) return cudaErrorInvalidValue;   // shape built without mom
     P.splits = sh.splits;
     P.cols_per_split = sh.cols_per_split;

@@ -45,7 +45,7 @@ constexpr int ROWS = TPB * RPT;   // output rows per CTA (RPT variant)
 constexpr int CHUNK = 256;        // columns per shared-memory tile (d <= 3)
 constexpr int KC = 4;             // columns per online-max sub-chunk
 constexpr int MAXD_PACKED = 3;    // packed fast path: d <= 3
-constexpr int MAXD = 64;          // generic path: d <= 64
+constexpr int MAXD = 256;         // generic path: d <= 256
 constexpr int CHUNK_G = 32;       // columns per tile on the generic path
 constexpr double LOG2E = 1.4426950408889634074;
 constexpr double LN2 = 0.69314718055994530942;
@@ -157,6 +157,13 @@ struct PassParams {
     unsigned int *rb_ticket;    // [row blocks]
     unsigned int *grid_ticket;  // [1]
     double *blk;                // [row blocks][4] block partial scalars
+    // feature-cost path (p = 2, tensor cores): both clouds pre-split into bf16
+    // pieces in the tile layout the MMA reads; null = the FP64 pair loops
+    const uint16_t *fx;         // pieces of the output-row points
+    const uint16_t *fy;         // pieces of the column points
+    const double *xn, *yn;      // squared norms |x|^2, |y|^2 (FP64)
+    int fkb;                    // 64-wide K blocks per point
+    int fpieces;                // bf16 pieces per value: 2 (BF16x3) or 3 (BF16x6)
 };
 
 // 2^x on the MUFU pipe (PTX ex2.approx.ftz.f32: relative error ~2^-22, results
@@ -877,6 +884,113 @@ __device__ __forceinline__ void tile_lse_packed(const PassParams &P, double alph
     }
 }
 
+// Per-row epilogue of a reduction pass (one thread per output row, R rows per
+// thread) and the grid-level finish step run by the last CTA of the grid.
+template <int ACC, int R>
+__device__ __forceinline__ void row_epilogue(const PassParams &P, int rb, int row_base, double beta,
+                                             const double (&Mv)[R], const double (&Sv)[R],
+                                             const double (&MOMv)[R], const double (&Hv)[R],
+                                             double *red, int &s_last) {
+    Ctl *ctl = P.ctl;
+    double acc4[4] = {0.0, 0.0, 0.0, 0.0};
+    double amax = -INFINITY;
+    double en = 0.0;
+    if (P.lamp_step == LAMP_A) { double sn; lamp_next(ctl->eta_t, ctl->s_t, ctl->tau_p, ctl->eta_lamp, en, sn); }
+    else if (P.lamp_step == LAMP_B) en = ctl->eta_next;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int o = row_base + threadIdx.x + r * TPB;
+        if (o >= P.n) continue;
+        if (ACC != ACC_LSE) {
+            if (P.out) P.out[o] = Mv[r];
+            amax = fmax(amax, Mv[r]);
+            if (P.marg) acc4[0] += P.marg[o] * Mv[r];
+            continue;
+        }
+        // natural-log LSE of the row: ln2 * (H + M + log2 S)
+        const double L = LN2 * (Hv[r] + Mv[r] + log2(Sv[r]));
+        const double Ec = (Sv[r] > 0.0) ? MOMv[r] / Sv[r] : 0.0;   // softmax-weighted mean cost
+        switch (P.epi) {
+            case EPI_SK_ROW: {
+                const double v = log(P.marg[o]) - L;
+                P.out[o] = v;
+                acc4[0] += P.marg[o] * v;
+                break;
+            }
+            case EPI_SK_RESID: {
+                const double mass = exp(P.rowpot[o] + L);
+                const double res = P.marg[o] - mass;
+                if (P.out) P.out[o] = res;
+                if (P.out2) P.out2[o] = mass * Ec;
+                acc4[0] += fabs(res);
+                acc4[1] += mass * Ec;
+                acc4[2] += P.marg[o] * P.rowpot[o];
+                break;
+            }
+            case EPI_LOGZ: {
+                if (P.out) P.out[o] = L;
+                if (P.marg) {
+                    if (P.aux) P.aux[o] = log(P.marg[o]) - L;
+                    acc4[0] += P.marg[o] * L;
+                }
+                break;
+            }
+            case EPI_SPP_COL: {
+                const double rp = P.rowpot ? P.rowpot[o] : 0.0;
+                const double res = exp(((beta == 0.0) ? 0.0 : beta * rp) + L);
+                const double cst = res * Ec;
+                if (P.out) P.out[o] = res;
+                if (P.out2) P.out2[o] = cst;
+                const double cj = P.cvec ? P.cvec[o] : 0.0;
+                acc4[0] += fabs(res - cj);
+                acc4[1] += cst;
+                acc4[2] += res * rp;
+                if (P.lamp_step == LAMP_A) {
+                    const double th = P.theta[o];
+                    acc4[3] += cj * th;
+                    P.thetab[o] = theta_step(th, res, cj, P.eta_mu_i[o], P.eta_mu_exp, 0, P.minv, P.maxv, 1.0);
+                    P.nub[o] = (1.0 - en) * P.nu[o] + en * th;
+                } else if (P.lamp_step == LAMP_B) {
+                    P.theta[o] = theta_step(P.theta[o], res, cj, P.eta_mu_i[o], P.eta_mu_exp, 1, P.minv, P.maxv, 1.0);
+                    P.nu[o] = (1.0 - en) * P.nu[o] + en * P.thetab[o];
+                }
+                break;
+            }
+            default:
+                if (P.out) P.out[o] = L;
+                break;
+        }
+    }
+
+    if (P.finish == FIN_NONE) return;
+    if (ACC == ACC_MAX) {
+        const double bm = block_max1(amax, red);
+        acc4[0] = bm;
+    } else {
+        block_sum4(acc4, red);
+    }
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 4; ++k) P.blk[rb * 4 + k] = acc4[k];
+        __threadfence();
+        const unsigned t = atomicAdd(P.grid_ticket, 1u);
+        s_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        __threadfence();
+        double tot[4] = {0.0, 0.0, 0.0, 0.0};
+        if (ACC == ACC_MAX) tot[0] = -INFINITY;
+        for (int b = 0; b < (int)gridDim.x; ++b) {
+            const volatile double *bb = P.blk + b * 4;
+            if (ACC == ACC_MAX) tot[0] = fmax(tot[0], bb[0]);
+            else for (int k = 0; k < 4; ++k) tot[k] += bb[k];
+        }
+        if (P.finish == FIN_LAMP_A) ctl->sum_c_theta = tot[3];
+        run_finish(P, tot);
+        *P.grid_ticket = 0u;
+    }
+}
+
 // FR: this instantiation tries the fixed-reference loop first (P.use_ref must be
 // set) and carries a compact online loop for its fallbacks; FR == false runs
 // the online loop alone, fully unrolled.
@@ -1004,104 +1118,7 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
         }
     }
 
-    // ---------------- epilogue: one thread per output row
-    double acc4[4] = {0.0, 0.0, 0.0, 0.0};
-    double amax = -INFINITY;
-    double en = 0.0;
-    if (P.lamp_step == LAMP_A) { double sn; lamp_next(ctl->eta_t, ctl->s_t, ctl->tau_p, ctl->eta_lamp, en, sn); }
-    else if (P.lamp_step == LAMP_B) en = ctl->eta_next;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int o = row_base + threadIdx.x + r * TPB;
-        if (o >= P.n) continue;
-        if (ACC != ACC_LSE) {
-            if (P.out) P.out[o] = Mv[r];
-            amax = fmax(amax, Mv[r]);
-            if (P.marg) acc4[0] += P.marg[o] * Mv[r];
-            continue;
-        }
-        // natural-log LSE of the row: ln2 * (H + M + log2 S)
-        const double L = LN2 * (Hv[r] + Mv[r] + log2(Sv[r]));
-        const double Ec = (Sv[r] > 0.0) ? MOMv[r] / Sv[r] : 0.0;   // softmax-weighted mean cost
-        switch (P.epi) {
-            case EPI_SK_ROW: {
-                const double v = log(P.marg[o]) - L;
-                P.out[o] = v;
-                acc4[0] += P.marg[o] * v;
-                break;
-            }
-            case EPI_SK_RESID: {
-                const double mass = exp(P.rowpot[o] + L);
-                const double res = P.marg[o] - mass;
-                if (P.out) P.out[o] = res;
-                if (P.out2) P.out2[o] = mass * Ec;
-                acc4[0] += fabs(res);
-                acc4[1] += mass * Ec;
-                acc4[2] += P.marg[o] * P.rowpot[o];
-                break;
-            }
-            case EPI_LOGZ: {
-                if (P.out) P.out[o] = L;
-                if (P.marg) {
-                    if (P.aux) P.aux[o] = log(P.marg[o]) - L;
-                    acc4[0] += P.marg[o] * L;
-                }
-                break;
-            }
-            case EPI_SPP_COL: {
-                const double rp = P.rowpot ? P.rowpot[o] : 0.0;
-                const double res = exp(((beta == 0.0) ? 0.0 : beta * rp) + L);
-                const double cst = res * Ec;
-                if (P.out) P.out[o] = res;
-                if (P.out2) P.out2[o] = cst;
-                const double cj = P.cvec ? P.cvec[o] : 0.0;
-                acc4[0] += fabs(res - cj);
-                acc4[1] += cst;
-                acc4[2] += res * rp;
-                if (P.lamp_step == LAMP_A) {
-                    const double th = P.theta[o];
-                    acc4[3] += cj * th;
-                    P.thetab[o] = theta_step(th, res, cj, P.eta_mu_i[o], P.eta_mu_exp, 0, P.minv, P.maxv, 1.0);
-                    P.nub[o] = (1.0 - en) * P.nu[o] + en * th;
-                } else if (P.lamp_step == LAMP_B) {
-                    P.theta[o] = theta_step(P.theta[o], res, cj, P.eta_mu_i[o], P.eta_mu_exp, 1, P.minv, P.maxv, 1.0);
-                    P.nu[o] = (1.0 - en) * P.nu[o] + en * P.thetab[o];
-                }
-                break;
-            }
-            default:
-                if (P.out) P.out[o] = L;
-                break;
-        }
-    }
-
-    if (P.finish == FIN_NONE) return;
-    if (ACC == ACC_MAX) {
-        const double bm = block_max1(amax, red);
-        acc4[0] = bm;
-    } else {
-        block_sum4(acc4, red);
-    }
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < 4; ++k) P.blk[rb * 4 + k] = acc4[k];
-        __threadfence();
-        const unsigned t = atomicAdd(P.grid_ticket, 1u);
-        s_last = (t == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (s_last && threadIdx.x == 0) {
-        __threadfence();
-        double tot[4] = {0.0, 0.0, 0.0, 0.0};
-        if (ACC == ACC_MAX) tot[0] = -INFINITY;
-        for (int b = 0; b < (int)gridDim.x; ++b) {
-            const volatile double *bb = P.blk + b * 4;
-            if (ACC == ACC_MAX) tot[0] = fmax(tot[0], bb[0]);
-            else for (int k = 0; k < 4; ++k) tot[k] += bb[k];
-        }
-        if (P.finish == FIN_LAMP_A) ctl->sum_c_theta = tot[3];
-        run_finish(P, tot);
-        *P.grid_ticket = 0u;
-    }
+    row_epilogue<ACC, R>(P, rb, row_base, beta, Mv, Sv, MOMv, Hv, red, s_last);
 }
 
 }  // namespace culamp_dev

@@ -62,6 +62,7 @@ struct LaunchShape {
     int cols_per_split;
     size_t smem;       // dynamic shared memory bytes
     size_t part_bytes; // split scratch bytes
+    int sms;           // SM count the shape was made for
 };
 
 // Grid and scratch requirement of a pass over n output rows and m columns.
@@ -74,6 +75,26 @@ cudaError_t launch_pass(PassParams P, int pmode, int acc, const LaunchShape &sh,
                         cudaStream_t st);
 
 int pmode_of(double p);   // P_L1 / P_SQ / P_INF / P_GEN
+
+// ---- feature-cost path (feature.cu): p = 2, d >= FEAT_MIN_D, tensor cores
+constexpr int FEAT_MIN_D = 32;
+
+struct FeatShape {
+    int rtiles, ctiles;   // 128-row tiles of the output rows, 128-column tiles
+    int splits, tps;      // column slices, column tiles per slice
+    int units, grid;      // work units (row tile x slice), CTAs (<= SMs)
+    int merge_rb;         // CTAs of the merge / epilogue kernel
+    size_t part_bytes;    // partials: splits * n * 3 doubles
+};
+
+FeatShape feat_shape(int n, int m, int sm_count);
+int feat_kblocks(int d);
+size_t feat_piece_elems(int n, int d, int pieces);   // bf16 elements of one packed cloud
+// Pack one cloud (n x d, FP64) into `pieces` bf16 pieces and its squared norms.
+cudaError_t feat_prepare(uint16_t *pieces, double *norms, const double *X, int n, int d, int np,
+                         cudaStream_t st);
+// Reduction on the tensor cores + merge / epilogue; P.fx .. P.fpieces set.
+cudaError_t launch_feat_pass(PassParams P, int acc, Scratch &scr, int sm_count, cudaStream_t st);
 
 }  // namespace culamp_host
 

@@ -63,11 +63,11 @@ enum SolverKind { KIND_SK = 1, KIND_LAMP = 2 };
 
 // Everything a captured graph bakes into kernel parameters.
 struct GraphKey {
-    int kind = 0, n = 0, m = 0, d = 0, pm_iter = 0, pm_resid = 0, unroll = 0;
+    int kind = 0, n = 0, m = 0, d = 0, pm_iter = 0, pm_resid = 0, unroll = 0, feat = 0;
     double p = 0, winf = 0, B = 0, eta_mu = 0;
     long long generation = -1;
     bool operator==(const GraphKey &o) const {
-        return kind == o.kind && n == o.n && m == o.m && d == o.d && pm_iter == o.pm_iter &&
+        return kind == o.kind && n == o.n && m == o.m && d == o.d && pm_iter == o.pm_iter && feat == o.feat &&
                pm_resid == o.pm_resid && unroll == o.unroll && generation == o.generation &&
                std::memcmp(&p, &o.p, sizeof(double)) == 0 && std::memcmp(&winf, &o.winf, sizeof(double)) == 0 &&
                std::memcmp(&B, &o.B, sizeof(double)) == 0 && std::memcmp(&eta_mu, &o.eta_mu, sizeof(double)) == 0;
@@ -80,6 +80,11 @@ struct culamp_handle_s::Solver {
     DevBuf X, Y, r, c, phi, psi, res, cost, logz, aux, nu, nub, theta, thetab, eta_mu, tmp, ctl,
         logbuf, setup, ws_phi, ws_psi, prev_phi, prev_psi;
     DevBuf hx, hy;             // host-variant staging (device side)
+    // feature-cost path: both clouds as bf16 pieces in the MMA tile image + norms
+    DevBuf fx, fy, fxn, fyn;
+    int feat_np = 0;           // pieces reserved for (0: feature path off)
+    int feat_kb = 0;           // K blocks of the packed clouds
+    bool feat_active = false;  // the staged inputs are packed and the path is on
     Scratch scr;
     cudaStream_t cap_stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -95,7 +100,7 @@ struct culamp_handle_s::Solver {
         drop_graphs();
         DevBuf *all[] = {&X, &Y, &r, &c, &phi, &psi, &res, &cost, &logz, &aux, &nu, &nub, &theta,
                          &thetab, &eta_mu, &tmp, &ctl, &logbuf, &setup, &ws_phi, &ws_psi,
-                         &prev_phi, &prev_psi, &hx, &hy};
+                         &prev_phi, &prev_psi, &hx, &hy, &fx, &fy, &fxn, &fyn};
         for (DevBuf *b : all) b->release();
         scr.release();
         if (cap_stream) cudaStreamDestroy(cap_stream);
@@ -118,7 +123,13 @@ namespace {
 
 using Solver = culamp_handle_s::Solver;
 
-int ensure_solver(culamp_handle h, int n, int m, int d, int64_t log_cap) {
+// bf16 pieces per feature value for these inputs and flags (0: pair loops).
+int feat_pieces(int d, uint32_t flags) {
+    if (d < FEAT_MIN_D || (flags & CULAMP_FLAG_FEAT_FP64)) return 0;
+    return (flags & CULAMP_FLAG_FEAT_X6) ? 3 : 2;
+}
+
+int ensure_solver(culamp_handle h, int n, int m, int d, int64_t log_cap, int feat_np = 0) {
     if (!h->solver) {
         h->solver = new (std::nothrow) Solver();
         if (!h->solver) return culamp_set_error(h, CULAMP_ERR_ALLOC, "solver state");
@@ -133,7 +144,7 @@ int ensure_solver(culamp_handle h, int n, int m, int d, int64_t log_cap) {
                                    S.res.ptr, S.cost.ptr, S.logz.ptr, S.aux.ptr, S.nu.ptr,
                                    S.nub.ptr, S.theta.ptr, S.thetab.ptr, S.eta_mu.ptr, S.tmp.ptr,
                                    S.ctl.ptr, S.logbuf.ptr, S.scr.part.ptr, S.scr.tickets.ptr,
-                                   S.scr.blk.ptr};
+                                   S.scr.blk.ptr, S.fx.ptr, S.fy.ptr, S.fxn.ptr, S.fyn.ptr};
     };
     const std::vector<void *> before = ptrs();
     cudaError_t e = cudaSuccess;
@@ -163,6 +174,14 @@ int ensure_solver(culamp_handle h, int n, int m, int d, int64_t log_cap) {
     R(S.ctl, sizeof(Ctl), true);
     R(S.setup, (8 + 2 * MAXD) * sizeof(double));
     R(S.logbuf, (size_t)(log_cap > 1 ? log_cap : 1) * sizeof(culamp_log_row));
+    if (feat_np > 0) {
+        R(S.fx, feat_piece_elems(n, d, feat_np) * sizeof(uint16_t));
+        R(S.fy, feat_piece_elems(m, d, feat_np) * sizeof(uint16_t));
+        R(S.fxn, (size_t)n * sizeof(double));
+        R(S.fyn, (size_t)m * sizeof(double));
+    }
+    S.feat_np = feat_np;
+    S.feat_active = false;
     // scratch for both pass orientations
     size_t pb = 0, nrb = 0;
     for (int mom = 0; mom < 2; ++mom)
@@ -171,6 +190,11 @@ int ensure_solver(culamp_handle h, int n, int m, int d, int64_t log_cap) {
                                       pass_shape(n, m, d, ACC_MAX, h->sm_count)}) {
             pb = sh.part_bytes > pb ? sh.part_bytes : pb;
             nrb = (size_t)sh.rb > nrb ? (size_t)sh.rb : nrb;
+        }
+    if (feat_np > 0)
+        for (const FeatShape &fs : {feat_shape(n, m, h->sm_count), feat_shape(m, n, h->sm_count)}) {
+            pb = fs.part_bytes > pb ? fs.part_bytes : pb;
+            nrb = (size_t)fs.merge_rb > nrb ? (size_t)fs.merge_rb : nrb;
         }
     if (e == cudaSuccess) e = S.scr.reserve(pb, nrb);
     if (e != cudaSuccess) return culamp_set_error(h, CULAMP_ERR_ALLOC, "workspace: %s", cudaGetErrorString(e));
@@ -302,6 +326,30 @@ int stage_inputs(culamp_handle h, const double *x, const double *y, int n, int m
     return CULAMP_OK;
 }
 
+// Pack the staged clouds for the tensor-core path when it was reserved and the
+// kept dimension count still qualifies.
+int prepare_features(culamp_handle h, int n, int m, int d_eff, cudaStream_t st) {
+    Solver &S = *h->solver;
+    S.feat_active = false;
+    if (S.feat_np <= 0 || d_eff < FEAT_MIN_D) return CULAMP_OK;
+    CUDA_TRY(h, feat_prepare(S.fx.as<uint16_t>(), S.fxn.as<double>(), S.X.as<double>(), n, d_eff, S.feat_np, st));
+    CUDA_TRY(h, feat_prepare(S.fy.as<uint16_t>(), S.fyn.as<double>(), S.Y.as<double>(), m, d_eff, S.feat_np, st));
+    S.feat_kb = feat_kblocks(d_eff);
+    S.feat_active = true;
+    return CULAMP_OK;
+}
+
+// Route a squared-Euclidean pass to the tensor-core feature path.
+void apply_feat(const Solver &S, PassParams &P, bool rows_are_x) {
+    if (!S.feat_active || pmode_of(P.pexp) != P_SQ) return;
+    P.fx = rows_are_x ? S.fx.as<uint16_t>() : S.fy.as<uint16_t>();
+    P.fy = rows_are_x ? S.fy.as<uint16_t>() : S.fx.as<uint16_t>();
+    P.xn = rows_are_x ? S.fxn.as<double>() : S.fyn.as<double>();
+    P.yn = rows_are_x ? S.fyn.as<double>() : S.fxn.as<double>();
+    P.fkb = S.feat_kb;
+    P.fpieces = S.feat_np;
+}
+
 PassParams mk(const double *X, const double *Y, int n, int m, int d, double p, Ctl *ctl) {
     PassParams P;
     std::memset(&P, 0, sizeof(P));
@@ -397,6 +445,9 @@ SkPlan make_sk_plan(culamp_handle h, int n, int m, int d, double p, uint32_t fla
     pl.k3.want_moment = 1;
     pl.k3.gate = GATE_CHECK;
     pl.k3.finish = FIN_SK_CHECK;
+    apply_feat(S, pl.k1, true);
+    apply_feat(S, pl.k2, false);
+    apply_feat(S, pl.k3, true);
     pl.s_rows = pass_shape(n, m, d, ACC_LSE, h->sm_count);
     pl.s_cols = pass_shape(m, n, d, ACC_LSE, h->sm_count);
     pl.s_rows_mom = pass_shape(n, m, d, ACC_LSE, h->sm_count, true);
@@ -445,6 +496,7 @@ int sinkhorn_loop(culamp_handle h, int n, int m, int d, double p, double eta, do
         key.n = n; key.m = m; key.d = d;
         key.pm_iter = pl.pm_iter; key.pm_resid = pl.pm_resid;
         key.p = p;
+        key.feat = S.feat_active ? S.feat_np : 0;
         key.unroll = pick_unroll((double)n * m * (frequency == 1 ? 3.0 : 2.0));
         key.generation = S.generation;
         cudaGraphExec_t ex = nullptr;
@@ -498,13 +550,15 @@ extern "C" int culamp_sinkhorn(culamp_handle h, const double *x, const double *y
     if (flags & CULAMP_FLAG_FORM_PLAIN)
         return culamp_plain_sinkhorn(h, x, y, n, m, d, r, c, args, frequency, p, phi0, psi0, flags,
                                      phi, psi, stats, log, log_cap, st);
-    s = ensure_solver(h, (int)n, (int)m, d, log ? log_cap : 0);
+    s = ensure_solver(h, (int)n, (int)m, d, log ? log_cap : 0, feat_pieces(d, flags));
     if (s) return s;
     Solver &S = *h->solver;
     int dk = d;
     s = stage_inputs(h, x, y, (int)n, (int)m, d, r, c, st, nullptr, &dk);
     if (s) return s;
     d = dk;
+    s = prepare_features(h, (int)n, (int)m, d, st);
+    if (s) return s;
     if (phi0) CUDA_TRY(h, cudaMemcpyAsync(S.phi.ptr, phi0, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     else CUDA_TRY(h, cudaMemsetAsync(S.phi.ptr, 0, n * sizeof(double), st));
     if (psi0) CUDA_TRY(h, cudaMemcpyAsync(S.psi.ptr, psi0, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -567,6 +621,7 @@ LampPlan make_lamp_plan(culamp_handle h, int n, int m, int d, double p, double w
     pl.k1.aux = S.aux.as<double>();
     pl.k1.use_ref = 1;
     pl.k1.finish = FIN_LAMP_Z;
+    apply_feat(S, pl.k1, true);
     // K2: column residual at nu (+ cost on check iterations), fused theta_bar / nu_bar step
     pl.k2 = mk(Y, X, m, n, d, p, ctl);
     pl.k2.ctr = X;
@@ -591,6 +646,7 @@ LampPlan make_lamp_plan(culamp_handle h, int n, int m, int d, double p, double w
     pl.k2.minv = minv;
     pl.k2.maxv = maxv;
     pl.k2.finish = FIN_LAMP_A;
+    apply_feat(S, pl.k2, false);
     // the same pass with the cost moment, on check iterations only
     pl.k2m = pl.k2;
     pl.k2m.want_moment = 1;
@@ -613,6 +669,7 @@ LampPlan make_lamp_plan(culamp_handle h, int n, int m, int d, double p, double w
         pl.kd.coef_mode = COEF_SPP_DUAL;
         pl.kd.use_ref = 1;
     }
+    apply_feat(S, pl.kd, true);
     // K3: logZ at nu_bar with (eta_t', s')
     pl.k3 = pl.k1;
     pl.k3.coef_mode = COEF_SPP_NEXT;
@@ -648,7 +705,7 @@ extern "C" int culamp_lamp(culamp_handle h, const double *x, const double *y, in
     if (flags & CULAMP_FLAG_FORM_PLAIN)
         return culamp_plain_lamp(h, x, y, n, m, d, r, c, args, frequency, p, flags, nu, phi, psi,
                                  theta, stats, log, log_cap, st);
-    s = ensure_solver(h, (int)n, (int)m, d, log ? log_cap : 0);
+    s = ensure_solver(h, (int)n, (int)m, d, log ? log_cap : 0, feat_pieces(d, flags));
     if (s) return s;
     Solver &S = *h->solver;
     double sum_rlogr = 0.0;
@@ -656,6 +713,8 @@ extern "C" int culamp_lamp(culamp_handle h, const double *x, const double *y, in
     s = stage_inputs(h, x, y, (int)n, (int)m, d, r, c, st, &sum_rlogr, &dk);
     if (s) return s;
     d = dk;
+    s = prepare_features(h, (int)n, (int)m, d, st);
+    if (s) return s;
     double winf = 0.0;
     s = compute_winf(h, (int)n, (int)m, d, p, st, &winf);
     if (s) return s;
@@ -715,6 +774,7 @@ extern "C" int culamp_lamp(culamp_handle h, const double *x, const double *y, in
         key.n = (int)n; key.m = (int)m; key.d = d;
         key.pm_iter = pl.pm;
         key.pm_resid = pl.dual_min ? 1 : 0;
+        key.feat = S.feat_active ? S.feat_np : 0;
         key.unroll = pick_unroll((double)n * m * 4.0);
         key.generation = S.generation;
         key.p = p;
@@ -802,13 +862,15 @@ extern "C" int culamp_annealed_sinkhorn(culamp_handle h, const double *x, const 
     if (flags & CULAMP_FLAG_FORM_PLAIN)
         return culamp_set_error(h, CULAMP_ERR_UNSUPPORTED, "annealed Sinkhorn has no plain form");
     cudaStream_t st = (cudaStream_t)stream;
-    s = ensure_solver(h, (int)n, (int)m, d, 0);
+    s = ensure_solver(h, (int)n, (int)m, d, 0, feat_pieces(d, flags));
     if (s) return s;
     Solver &S = *h->solver;
     int dk = d;
     s = stage_inputs(h, x, y, (int)n, (int)m, d, r, c, st, nullptr, &dk);
     if (s) return s;
     d = dk;
+    s = prepare_features(h, (int)n, (int)m, d, st);
+    if (s) return s;
     double winf = 0.0;
     s = compute_winf(h, (int)n, (int)m, d, p, st, &winf);
     if (s) return s;

@@ -27,6 +27,8 @@ FLAG_CHECK_ALWAYS = 2
 FLAG_MARGINAL_ONLY = 4
 FLAG_FORM_PLAIN = 8
 FLAG_NO_GRAPH = 16
+FLAG_FEAT_X6 = 32
+FLAG_FEAT_FP64 = 64
 
 
 class CulampError(RuntimeError):

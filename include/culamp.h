@@ -51,6 +51,11 @@ extern "C" {
                                           (warp per row, FP32 potentials, host-synchronised
                                           loop). Default is the chosen form.               */
 #define CULAMP_FLAG_NO_GRAPH      16u  /* chosen form without CUDA graphs (debugging)      */
+#define CULAMP_FLAG_FEAT_X6       32u  /* feature clouds (d >= 32, squared cost): BF16x6
+                                          split products (3 bf16 pieces, ~24-bit products)
+                                          instead of the default BF16x3 (2 pieces)          */
+#define CULAMP_FLAG_FEAT_FP64     64u  /* feature clouds on the FP64 pair loops instead of
+                                          the tensor cores (exact inner products, slow)     */
 
 /* EOTArgs (src/Utilities.jl:18-31), same field names and defaults. */
 typedef struct culamp_args {

@@ -315,14 +315,54 @@ def np_lse(a, axis):
     return (np.log(np.exp(a - mx).sum(axis=axis, keepdims=True)) + mx).squeeze(axis)
 
 
+def bf16_rn(a):
+    """Nearest bf16 value (ties to even) of each FP64 entry, as FP64: keep 7 of
+    the 52 stored mantissa bits, rounding on the bit pattern."""
+    b = np.ascontiguousarray(a, np.float64).copy().view(np.uint64)
+    b = (b + np.uint64((1 << 44) - 1) + ((b >> np.uint64(45)) & np.uint64(1))) & ~np.uint64((1 << 45) - 1)
+    return b.view(np.float64)
+
+
+def bf16_pieces(a, pieces):
+    """a = a_0 + a_1 + ... + rest: a_k is the bf16 rounding of what a_0..a_{k-1} leave."""
+    out, rest = [], np.asarray(a, np.float64).copy()
+    for _ in range(pieces):
+        h = bf16_rn(rest)
+        out.append(h)
+        rest = rest - h
+    return out
+
+
+def split_dot(x, y, pieces):
+    """<x_i, y_j> from bf16 pieces with FP64 sums: pieces=2 is BF16x3
+    (x0y0 + x0y1 + x1y0), pieces=3 is BF16x6 (+ x0y2 + x1y1 + x2y0)."""
+    xs, ys = bf16_pieces(x, pieces), bf16_pieces(y, pieces)
+    dot = np.zeros((len(x), len(y)))
+    for a in range(pieces):
+        for b in range(pieces - a):
+            dot += xs[a] @ ys[b].T
+    return dot
+
+
+def feature_cost(x, y, pieces=None):
+    """Squared Euclidean cost |x|^2 + |y|^2 - 2<x, y> with exact FP64 norms and
+    the inner products exact (pieces=None) or from bf16 split products."""
+    x, y = np.asarray(x, np.float64), np.asarray(y, np.float64)
+    dot = x @ y.T if pieces is None else split_dot(x, y, pieces)
+    return (x * x).sum(1)[:, None] + (y * y).sum(1)[None, :] - 2.0 * dot
+
+
 def np_sinkhorn_kernel(x, y, r, c, eta_p, itermax, frequency=1, epsilon=0.0, p=2.0,
-                       true_pinf=False, phi0=None, psi0=None):
-    """Sinkhorn of SinkhornKernel.jl:477-559 restated with dense numpy arrays."""
-    winf = np_cost(x, y, p).max()
+                       true_pinf=False, phi0=None, psi0=None, cost=None, winf=None):
+    """Sinkhorn of SinkhornKernel.jl:477-559 restated with dense numpy arrays.
+    `cost` replaces the pair cost of the iterations and the residual (p = 2
+    only), `winf` the normaliser max_ij C_ij."""
+    if winf is None:
+        winf = np_cost(x, y, p).max()
     ip = 2.0 if (math.isinf(p) and not true_pinf) else p
     rp = p if true_pinf else (1.0 if p == 1 else 2.0)
-    Ci = np_cost(x, y, ip)
-    Cr = np_cost(x, y, rp)
+    Ci = np_cost(x, y, ip) if cost is None else cost
+    Cr = np_cost(x, y, rp) if cost is None else cost
     phi = np.zeros(len(r)) if phi0 is None else np.array(phi0, np.float64)
     psi = np.zeros(len(c)) if psi0 is None else np.array(psi0, np.float64)
     k = -1.0 / (eta_p * winf)
@@ -345,10 +385,11 @@ def np_theta_update(theta0, res, c, eta_mu_i, eta_mu, adjust, minv, maxv):
 
 
 def np_lamp_kernel(x, y, r, c, eta_p, itermax, p=2.0, alpha=0.01, tau_mu=1.0, eta_mu=0.0,
-                   B=1.0):
-    """LAMP of MirrorProxKernel.jl:1019-1132 (non-verbose: runs itermax)."""
-    C_ = np_cost(x, y, p)
-    winf = C_.max()
+                   B=1.0, cost=None, winf=None):
+    """LAMP of MirrorProxKernel.jl:1019-1132 (non-verbose: runs itermax).
+    `cost` / `winf` as in np_sinkhorn_kernel."""
+    C_ = np_cost(x, y, p) if cost is None else cost
+    winf = C_.max() if winf is None else winf
     n, m = C_.shape
     eta = eta_p / (2 * winf)
     emu = (c + alpha / n) / tau_mu

@@ -123,3 +123,25 @@ def test_dense_solvers_converge(oracle, golden_dir):
     th, nu, _, st2, log2 = oracle.lamp_dense(g["W"], g["r"], g["c"], b, frequency=20)
     assert np.array_equal(nu, g["lamp_nu"])
     assert log2[-1][2] < log2[0][2]
+
+
+def test_bf16_split_emulation(oracle):
+    """The split-precision cost model of the tensor-core feature path: bf16
+    rounding matches torch's on float-representable inputs (ties to even), the
+    pieces reconstruct the value, and BF16x3 / BF16x6 inner products sit at
+    their expected error levels."""
+    import torch
+    g = np.random.default_rng(3)
+    a = g.uniform(-4, 4, 200000).astype(np.float32).astype(np.float64)
+    want = torch.from_numpy(a.astype(np.float32)).to(torch.bfloat16).to(torch.float64).numpy()
+    assert np.array_equal(oracle.bf16_rn(a), want)
+    v = g.uniform(0, 1, 5000)
+    p = oracle.bf16_pieces(v, 3)
+    assert np.abs(p[0] + p[1] + p[2] - v).max() <= 2.0 ** -24 * np.abs(v).max()
+    x, y = g.uniform(0, 1, (40, 256)), g.uniform(0, 1, (30, 256))
+    exact = x @ y.T
+    e3 = np.abs(oracle.split_dot(x, y, 2) - exact).max() / np.abs(exact).max()
+    e6 = np.abs(oracle.split_dot(x, y, 3) - exact).max() / np.abs(exact).max()
+    assert 1e-7 < e3 < 2e-5 and e6 < 1e-8
+    c = oracle.feature_cost(x, y)
+    assert np.allclose(c, ((x[:, None, :] - y[None, :, :]) ** 2).sum(-1), rtol=1e-12, atol=1e-12)
