@@ -52,7 +52,31 @@ def parse():
     ap.add_argument("--profile-pass", type=int, default=0, metavar="N",
                     help="only launch the fused row-LSE pass on an N-point RGB instance "
                          "(warmup + steps launches), for profiler captures")
+    ap.add_argument("--profile-feature", type=int, default=0, metavar="N",
+                    help="only run warmup + steps Sinkhorn iterations on an N-point d=256 "
+                         "feature instance (tensor-core path, pass by pass), for profiler captures")
     return ap.parse_args()
+
+
+def profile_feature(args):
+    """Profiler target for the tensor-core feature path: warmup + steps
+    Sinkhorn iterations on an N x N, d = 256 feature instance, launched pass by
+    pass (FLAG_NO_GRAPH). feat_reduce_kernel launches 3 times per iteration
+    (row pass, column pass, residual check -- the check returns at once except
+    on check iterations, here iteration 1 only), so `-k regex:feat_reduce -s 6
+    -c 1` captures the row pass of iteration 3."""
+    import torch
+    import culamp_b200 as cb
+    from culamp_b200 import datasets as D
+    n = args.profile_feature
+    x, y, r, c = D.feature_instance(n, n, 256)
+    X, Y, R, Cc = (torch.as_tensor(v, device="cuda") for v in (x, y, r, c))
+    a = cb.EOTArgs(eta_p=1e-2, epsilon=0.0, itermax=args.warmup + args.steps, verbose=False)
+    res = cb.solve_sinkhorn(X, Y, R, Cc, a, 10**6, 2.0, flags=cb.FLAG_NO_GRAPH)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_feature": n, "iterations": res.iterations,
+                      "finite": bool(torch.isfinite(res.phi).all())}))
+    return 0
 
 
 def profile_pass(args):
@@ -267,6 +291,8 @@ def main():
         return reference_arm(args)
     if args.profile_pass:
         return profile_pass(args)
+    if args.profile_feature:
+        return profile_feature(args)
 
     import numpy as np
     import torch
@@ -436,7 +462,42 @@ def extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_chosen, chosen_ms):
                             "iterations": s5.iterations, "fp64_row_l1": rl, "fp64_col_l1": cl,
                             "pass_ms": ms5, "pass_timing": how5,
                             "pass_gpair_s": 65536.0 ** 2 / (ms5 * 1e-3) / 1e9}
+    ex["features_16384_d256"] = feature_extra(cb, D, torch, dev)
     return ex
+
+
+def feature_extra(cb, D, torch, dev, n=16384, d=256):
+    """Feature-space OT: n = m = 16384 points in R^256 (log1p negative-binomial
+    counts, 90% zeros, rows L2-normalised), uniform marginals, eta_p = 1e-2,
+    squared Euclidean cost on the tensor cores. Per split form: time per
+    iteration over 20 iterations (two passes of 2*d*n*m useful FLOPs each), its
+    fraction of the tensor roofline (measured bf16 peak / products per useful
+    MAC), and a solve to 1e-6 L1 marginal error with the FP64-checked errors."""
+    x, y, r, c = D.feature_instance(n, n, d)
+    X, Y, R, Cc = (torch.as_tensor(v, device=dev) for v in (x, y, r, c))
+    peaks = load_peaks() or {}
+    peak = peaks.get("bf16_tflops") or 1590.0
+    out = {"n": n, "m": n, "d": d, "eta_p": 1e-2, "peak_bf16_tflops": peak,
+           "peak_source": "MEASURED_PEAKS.json bf16_tflops" if "bf16_tflops" in peaks else "fallback"}
+    useful = 2.0 * 2.0 * d * n * n      # FLOPs of the two inner-product passes of one iteration
+    for name, flag, prods in (("bf16x3", 0, 3), ("bf16x6", cb.FLAG_FEAT_X6, 6)):
+        a = cb.EOTArgs(eta_p=1e-2, epsilon=0.0, itermax=20, tmax=60.0, verbose=False)
+        cb.solve_sinkhorn(X, Y, R, Cc, a.copy(itermax=3), 10 ** 6, 2.0, flags=flag)
+        t = cb.solve_sinkhorn(X, Y, R, Cc, a, 10 ** 6, 2.0, flags=flag)
+        ms_it = t.elapsed_ms / max(1, t.iterations)
+        tf = useful / (ms_it * 1e-3) / 1e12
+        b = cb.EOTArgs(eta_p=1e-2, epsilon=6e-6, itermax=5000, tmax=60.0, verbose=False)
+        s = cb.solve_sinkhorn(X, Y, R, Cc, b, 10, 2.0, flags=flag)
+        rl, cl = cb.marginal_error_fp64(X, Y, R, Cc, s.phi, s.psi, 1e-2, s.winf, 2.0)
+        out[name] = {"ms_per_iter": ms_it, "useful_tflops": tf,
+                     "roofline_frac": tf / (peak / prods), "roofline": f"bf16 peak / {prods}",
+                     "solve_reached_tol": s.stopped == 1, "solve_ms": s.elapsed_ms,
+                     "iterations": s.iterations, "self_l1": s.residual,
+                     "fp64_row_l1": rl, "fp64_col_l1": cl}
+    a = cb.EOTArgs(eta_p=1e-2, epsilon=0.0, itermax=2, tmax=60.0, verbose=False)
+    t = cb.solve_sinkhorn(X, Y, R, Cc, a, 10 ** 6, 2.0, flags=cb.FLAG_FEAT_FP64)
+    out["fp64_pair_loops_ms_per_iter"] = t.elapsed_ms / max(1, t.iterations)
+    return out
 
 
 if __name__ == "__main__":
