@@ -56,7 +56,7 @@ static cudaError_t launch_t(const PassParams &P, const LaunchShape &sh, cudaStre
         if (e != cudaSuccess) return e;
     }
     dim3 grid(sh.rb, sh.splits);
-    kern<<<grid, TPB, sh.smem, st>>>(P);
+    kern<<<grid, TPB, sh.smem, st>>>(P, nullptr, nullptr, 0);
     return cudaGetLastError();
 }
 

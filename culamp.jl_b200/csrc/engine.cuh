@@ -164,6 +164,10 @@ struct PassParams {
     const double *xn, *yn;      // squared norms |x|^2, |y|^2 (FP64)
     int fkb;                    // 64-wide K blocks per point
     int fpieces;                // bf16 pieces per value: 2 (BF16x3) or 3 (BF16x6)
+    // batched launches: this instance's row blocks (pair passes) and work-unit
+    // geometry (feature passes: row tiles, column tiles, slices, tiles per slice)
+    int nrb;
+    int ft_rtiles, ft_ctiles, ft_splits, ft_tps;
 };
 
 // 2^x on the MUFU pipe (PTX ex2.approx.ftz.f32: relative error ~2^-22, results
@@ -890,7 +894,7 @@ template <int ACC, int R>
 __device__ __forceinline__ void row_epilogue(const PassParams &P, int rb, int row_base, double beta,
                                              const double (&Mv)[R], const double (&Sv)[R],
                                              const double (&MOMv)[R], const double (&Hv)[R],
-                                             double *red, int &s_last) {
+                                             double *red, int &s_last, int nrb) {
     Ctl *ctl = P.ctl;
     double acc4[4] = {0.0, 0.0, 0.0, 0.0};
     double amax = -INFINITY;
@@ -973,14 +977,14 @@ __device__ __forceinline__ void row_epilogue(const PassParams &P, int rb, int ro
         for (int k = 0; k < 4; ++k) P.blk[rb * 4 + k] = acc4[k];
         __threadfence();
         const unsigned t = atomicAdd(P.grid_ticket, 1u);
-        s_last = (t == gridDim.x - 1);
+        s_last = (t == (unsigned)nrb - 1u);
     }
     __syncthreads();
     if (s_last && threadIdx.x == 0) {
         __threadfence();
         double tot[4] = {0.0, 0.0, 0.0, 0.0};
         if (ACC == ACC_MAX) tot[0] = -INFINITY;
-        for (int b = 0; b < (int)gridDim.x; ++b) {
+        for (int b = 0; b < nrb; ++b) {
             const volatile double *bb = P.blk + b * 4;
             if (ACC == ACC_MAX) tot[0] = fmax(tot[0], bb[0]);
             else for (int k = 0; k < 4; ++k) tot[k] += bb[k];
@@ -994,11 +998,45 @@ __device__ __forceinline__ void row_epilogue(const PassParams &P, int rb, int ro
 // FR: this instantiation tries the fixed-reference loop first (P.use_ref must be
 // set) and carries a compact online loop for its fallbacks; FR == false runs
 // the online loop alone, fully unrolled.
-template <int PM, int D, int ACC, int R, bool MOM, bool FR>
-__global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassParams P) {
+// BAT == false: one pass, grid (row blocks, column splits), parameters P0.
+// BAT == true: the same pass over many independent instances in one launch:
+// CTA b belongs to the instance i with block_start[i] <= b < block_start[i+1]
+// and is its local block b - block_start[i] = sp * nrb + rb. Each instance
+// carries its own parameters (plist[i]), scratch, tickets and control block.
+template <int PM, int D, int ACC, int R, bool MOM, bool FR, bool BAT = false>
+__global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4)
+    pair_pass_kernel(const __grid_constant__ PassParams P0, const PassParams *plist,
+                     const int *block_start, int count) {
     extern __shared__ __align__(16) double smem[];
     __shared__ double red[4 * (TPB / 32)];
     __shared__ int s_last;
+    __shared__ int s_bat[3];                      // BAT: row block, split, row-block count
+    __shared__ __align__(16) PassParams sP;       // BAT: this instance's parameters
+    if constexpr (BAT) {
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = count - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (block_start[mid] <= (int)blockIdx.x) lo = mid;
+                else hi = mid - 1;
+            }
+            const int local = (int)blockIdx.x - block_start[lo];
+            const int nrb = plist[lo].nrb;
+            s_bat[0] = local % nrb;
+            s_bat[1] = local / nrb;
+            s_bat[2] = nrb;
+            s_last = lo;
+        }
+        __syncthreads();
+        const int *src = reinterpret_cast<const int *>(plist + s_last);
+        int *dst = reinterpret_cast<int *>(&sP);
+        for (int k = threadIdx.x; k < (int)(sizeof(PassParams) / sizeof(int)); k += TPB) dst[k] = src[k];
+        __syncthreads();
+    }
+    const PassParams &P = *(BAT ? &sP : &P0);
+#define CULAMP_RB (BAT ? s_bat[0] : (int)blockIdx.x)
+#define CULAMP_SP (BAT ? s_bat[1] : (int)blockIdx.y)
+#define CULAMP_NRB (BAT ? s_bat[2] : (int)gridDim.x)
     Ctl *ctl = P.ctl;
     if (ctl) {
         if (ctl->stop) return;
@@ -1008,10 +1046,8 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
     double alpha = 0.0, beta = 0.0;
     if (ACC == ACC_LSE) resolve_coefs(P, alpha, beta);
 
-    const int rb = blockIdx.x;               // row block
-    const int sp = blockIdx.y;               // column split
-    const int row_base = rb * (TPB * R);
-    const int cbeg = sp * P.cols_per_split;
+    const int row_base = CULAMP_RB * (TPB * R);
+    const int cbeg = CULAMP_SP * P.cols_per_split;
     const int cend = min(P.m, cbeg + P.cols_per_split);
 
     double Mv[R], Sv[R], MOMv[R], Hv[R];
@@ -1053,7 +1089,7 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
         for (int r = 0; r < R; ++r) {
             const int row = row_base + threadIdx.x + r * TPB;
             if (row < P.n) {
-                double *pp = P.part + ((size_t)sp * P.n + row) * 3;
+                double *pp = P.part + ((size_t)CULAMP_SP * P.n + row) * 3;
                 pp[0] = Mv[r]; pp[1] = Sv[r];
                 if (MOM) pp[2] = MOMv[r];
             }
@@ -1061,7 +1097,7 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) {
-            const unsigned t = atomicAdd(&P.rb_ticket[rb], 1u);
+            const unsigned t = atomicAdd(&P.rb_ticket[CULAMP_RB], 1u);
             s_last = (t == (unsigned)(P.splits - 1));
         }
         __syncthreads();
@@ -1095,7 +1131,7 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
             }
             Mv[r] = M; Sv[r] = S; MOMv[r] = MO;
         }
-        if (threadIdx.x == 0) P.rb_ticket[rb] = 0u;   // re-arm for the next launch
+        if (threadIdx.x == 0) P.rb_ticket[CULAMP_RB] = 0u;   // re-arm for the next launch
     }
 
     if constexpr (FR && ACC == ACC_LSE && D > 0 && !MOM) {
@@ -1118,7 +1154,10 @@ __global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4) pair_pass_kernel(PassP
         }
     }
 
-    row_epilogue<ACC, R>(P, rb, row_base, beta, Mv, Sv, MOMv, Hv, red, s_last);
+    row_epilogue<ACC, R>(P, CULAMP_RB, row_base, beta, Mv, Sv, MOMv, Hv, red, s_last, CULAMP_NRB);
+#undef CULAMP_RB
+#undef CULAMP_SP
+#undef CULAMP_NRB
 }
 
 }  // namespace culamp_dev

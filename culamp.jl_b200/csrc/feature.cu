@@ -473,7 +473,7 @@ __global__ void __launch_bounds__(TPB) feat_merge_kernel(PassParams P) {
         MOMv[r] = MO;
         Hv[r] = (ACC == ACC_LSE && row < P.n) ? alpha * LOG2E * P.xn[row] : 0.0;
     }
-    row_epilogue<ACC, RPT>(P, rb, row_base, beta, Mv, Sv, MOMv, Hv, red, s_last);
+    row_epilogue<ACC, RPT>(P, rb, row_base, beta, Mv, Sv, MOMv, Hv, red, s_last, gridDim.x);
 }
 
 // Round to the nearest bf16 value, ties to even, on the FP64 bit pattern (keep
