@@ -417,6 +417,7 @@ def main():
 
     if rank == 0 and world == 1 and not args.no_extras:
         line["extras"] = extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_med, value)
+        line["extras"]["batched_512"] = batched_extra(cb, D, torch, np, dev, dfma, ex2)
         line["cpu_baseline"] = cpu_baseline(x, y, r, c, it_med, os.cpu_count() or 1)
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -464,6 +465,53 @@ def extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_chosen, chosen_ms):
                             "pass_gpair_s": 65536.0 ** 2 / (ms5 * 1e-3) / 1e9}
     ex["features_16384_d256"] = feature_extra(cb, D, torch, dev)
     return ex
+
+
+def batched_extra(cb, D, torch, np, dev, dfma, ex2, count=512, sample=24):
+    """Batched uneven solves: `count` instances, n and m log-uniform in [256,
+    8192], d in {2, 3, 64}, Gaussian-mixture points in [0,1]^d, Dirichlet(1)
+    marginals, squared Euclidean cost, eta_p = 1e-2, every instance to 1e-6 L1
+    marginal error (checked every 10 iterations), in one culamp_batched_sinkhorn
+    call (one graph launch). Reported beside it: the same instances solved one
+    by one with culamp_sinkhorn (the first `sample` timed, scaled to the batch
+    by pair count) and the weighted roofline -- each instance's pair passes at
+    its own bound (d <= 3: min(DFMA / (d + 1), ex2) pairs/s from the pipe
+    probes; d = 64: bf16 peak / 3 useful FLOP/s), summed, over the measured time."""
+    inst = D.batched_instances(count, lo=256, hi=8192, dims=(2, 3, 64), seed=0)
+    dinst = [tuple(torch.as_tensor(v, device=dev) for v in t) for t in inst]
+    a = cb.EOTArgs(eta_p=1e-2, epsilon=6e-6, itermax=20000, tmax=120.0, verbose=False)
+    t0 = time.perf_counter()
+    first = cb.solve_batched_sinkhorn(dinst, a, frequency=10, p=2.0)
+    first_wall = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    out = cb.solve_batched_sinkhorn(dinst, a, frequency=10, p=2.0)
+    wall = (time.perf_counter() - t0) * 1e3
+    peaks = load_peaks() or {}
+    bf16 = (peaks.get("bf16_tflops") or 1590.0) * 1e12
+    ideal_s, pairs_done = 0.0, 0.0
+    for (x, y, r, c), res in zip(inst, out.results):
+        n, m, d = x.shape[0], y.shape[0], x.shape[1]
+        pairs = 2.0 * n * m * res.iterations + n * m * (res.iterations // 10 + 1)
+        pairs_done += pairs
+        ideal_s += pairs * 2.0 * d * 3 / bf16 if d >= 32 else pairs / min(dfma / (d + 1), ex2)
+    seq_ms, seq_pairs = 0.0, 0.0
+    for (x, y, r, c) in dinst[:sample]:
+        one = cb.solve_sinkhorn(x, y, r, c, a, 10, 2.0)
+        seq_ms += one.elapsed_ms
+        seq_pairs += x.shape[0] * y.shape[0]
+    tot_pairs = sum(float(t[0].shape[0]) * t[1].shape[0] for t in inst)
+    its = [r.iterations for r in out.results]
+    return {"instances": count, "dims": [2, 3, 64], "eta_p": 1e-2, "tolerance": 1e-6,
+            "all_reached_tol": all(r.stopped == 1 for r in out.results),
+            "ms": out.elapsed_ms, "wall_ms": wall, "first_call_wall_ms": first_wall,
+            "first_call_tune_ms": first.tune_ms, "iterations_max": max(its),
+            "iterations_mean": float(np.mean(its)), "target_ctas_per_sm": out.target_ctas_per_sm,
+            "feat_tiles_per_unit": out.feat_tiles_per_unit, "unroll": out.unroll,
+            "launches_per_iteration": out.launches_per_iteration,
+            "gpair_s": pairs_done / (out.elapsed_ms * 1e-3) / 1e9,
+            "weighted_roofline_frac": ideal_s / (out.elapsed_ms * 1e-3),
+            "sequential_ms_estimate": seq_ms * tot_pairs / max(seq_pairs, 1.0),
+            "sequential_sample": sample}
 
 
 def feature_extra(cb, D, torch, dev, n=16384, d=256):

@@ -1,6 +1,8 @@
 // engine.cu -- template instantiations of the pair-pass kernel and the launcher.
 #include <cmath>
 
+#include <cstring>
+
 #include "internal.h"
 
 namespace culamp_host {
@@ -92,6 +94,65 @@ static cudaError_t launch_p(const PassParams &P, int pm, const LaunchShape &sh, 
         case P_SQ: return launch_d<P_SQ, ACC>(P, sh, st);
         case P_INF: return launch_d<P_INF, ACC>(P, sh, st);
         default: return launch_d<P_GEN, ACC>(P, sh, st);
+    }
+}
+
+template <int PM, int D, bool MOM, bool FR>
+static cudaError_t launch_b(const PassParams *plist, const int *block_start, int count, int total_blocks,
+                            size_t smem, cudaStream_t st) {
+    auto kern = pair_pass_kernel<PM, D, ACC_LSE, RPT, MOM, FR, true>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    PassParams dummy;
+    memset(&dummy, 0, sizeof(dummy));
+    kern<<<total_blocks, TPB, smem, st>>>(dummy, plist, block_start, count);
+    return cudaGetLastError();
+}
+
+template <int PM, int D>
+static cudaError_t launch_bd(const PassParams *plist, const int *block_start, int count, int total_blocks,
+                             size_t smem, bool mom, bool fr, cudaStream_t st) {
+    if (mom) return launch_b<PM, D, true, false>(plist, block_start, count, total_blocks, smem, st);
+    if (fr && D > 0) return launch_b<PM, D, false, (D > 0)>(plist, block_start, count, total_blocks, smem, st);
+    return launch_b<PM, D, false, false>(plist, block_start, count, total_blocks, smem, st);
+}
+
+template <int PM>
+static cudaError_t launch_bp(const PassParams *plist, const int *block_start, int count, int total_blocks,
+                             size_t smem, int d, bool mom, bool fr, cudaStream_t st) {
+    switch (d) {
+        case 1: return launch_bd<PM, 1>(plist, block_start, count, total_blocks, smem, mom, fr, st);
+        case 2: return launch_bd<PM, 2>(plist, block_start, count, total_blocks, smem, mom, fr, st);
+        case 3: return launch_bd<PM, 3>(plist, block_start, count, total_blocks, smem, mom, fr, st);
+        default: return launch_bd<PM, 0>(plist, block_start, count, total_blocks, smem, mom, fr, st);
+    }
+}
+
+cudaError_t launch_pass_batched(const PassParams *plist, const int *block_start, int count,
+                                int total_blocks, size_t smem, int pm, int d, int acc, bool mom,
+                                bool fixed_ref, cudaStream_t st) {
+    if (count < 1 || total_blocks < 1) return cudaSuccess;
+    if (acc != ACC_LSE) return cudaErrorInvalidValue;
+    if (pm == P_SQ) return launch_bp<P_SQ>(plist, block_start, count, total_blocks, smem, d, mom, fixed_ref, st);
+    if (pm == P_L1) return launch_bp<P_L1>(plist, block_start, count, total_blocks, smem, d, mom, fixed_ref, st);
+    return cudaErrorNotSupported;
+}
+
+cudaError_t launch_pass_at(PassParams P, int pm, int acc, const LaunchShape &sh, double *part,
+                           unsigned *tickets, double *blk, cudaStream_t st) {
+    if (P.want_moment && sh.R != RPT) return cudaErrorInvalidValue;
+    P.splits = sh.splits;
+    P.cols_per_split = sh.cols_per_split;
+    P.part = part;
+    P.rb_ticket = tickets;
+    P.grid_ticket = tickets + sh.rb;
+    P.blk = blk;
+    switch (acc) {
+        case ACC_LSE: return launch_p<ACC_LSE>(P, pm, sh, st);
+        case ACC_MAX: return launch_p<ACC_MAX>(P, pm, sh, st);
+        default: return launch_p<ACC_MIN>(P, pm, sh, st);
     }
 }
 

@@ -35,6 +35,8 @@
 // block records a device timeout.
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include "internal.h"
 
 namespace {
@@ -175,23 +177,50 @@ constexpr size_t ft_smem_bytes() {
     return 1024 + (size_t)FtCfg<NP>::NS * 2 * NP * FT_PIECE_BYTES + FT_CTRL_BYTES;
 }
 
+// Unit u's parameters: the kernel argument, or (batched) the instance i with
+// unit_start[i] <= u < unit_start[i + 1]; `local` = u's index in its instance.
+template <bool BAT>
+__device__ __forceinline__ const PassParams &unit_params(const PassParams &P0, const PassParams *plist,
+                                                        const int *unit_start, int count, int u,
+                                                        int &local) {
+    if (!BAT) {
+        local = u;
+        return P0;
+    }
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (unit_start[mid] <= u) lo = mid;
+        else hi = mid - 1;
+    }
+    local = u - unit_start[lo];
+    return plist[lo];
+}
+
+// The pass does not run for this instance now (solver stopped, or gated).
+__device__ __forceinline__ bool pass_skipped(const PassParams &Q) {
+    const Ctl *c = Q.ctl;
+    if (!c) return false;
+    if (c->stop) return true;
+    if (Q.gate == GATE_CHECK && !c->do_check) return true;
+    if (Q.gate == GATE_NOCHECK && c->do_check) return true;
+    return false;
+}
+
 // One CTA per SM; units (row tile, column-tile slice) strided over the grid.
-template <int NP, int ACC, bool MOM>
+// BAT: units of many instances (plist / unit_start, total_units in all);
+// otherwise the units of P0 (P0.ft_rtiles x P0.ft_splits).
+template <int NP, int ACC, bool MOM, bool BAT>
 __global__ void __launch_bounds__(FT_THREADS, 1)
-    feat_reduce_kernel(PassParams P, int rtiles, int ctiles, int splits, int tps) {
+    feat_reduce_kernel(const __grid_constant__ PassParams P0, const PassParams *plist,
+                       const int *unit_start, int count, int total_units, int *batch_err) {
     constexpr int NS = FtCfg<NP>::NS;
     constexpr int NPROD = FtCfg<NP>::NPROD;
     constexpr uint32_t STAGE = 2u * NP * FT_PIECE_BYTES;
     extern __shared__ unsigned char ft_raw[];
 
-    Ctl *ctl = P.ctl;
-    if (ctl) {
-        if (ctl->stop) return;
-        if (P.gate == GATE_CHECK && !ctl->do_check) return;
-        if (P.gate == GATE_NOCHECK && ctl->do_check) return;
-    }
-    double alpha = 0.0, beta = 0.0;
-    if (ACC == ACC_LSE) resolve_coefs(P, alpha, beta);
+    if (!BAT && pass_skipped(P0)) return;
+    const int units = BAT ? total_units : P0.ft_rtiles * P0.ft_splits;
 
     const uint32_t raw = smem_u32(ft_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;            // swizzle atoms need 1024-byte alignment
@@ -228,8 +257,6 @@ __global__ void __launch_bounds__(FT_THREADS, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(tmem_slot);
-    const int units = rtiles * splits;
-    const int nkb = P.fkb;
 
     if (warp == 0) {
         // ------------------------------------------------ producer
@@ -239,7 +266,12 @@ __global__ void __launch_bounds__(FT_THREADS, 1)
         for (int s = 0; s < NS; ++s) last_use[s] = -1;
         bool ok = true;
         for (int u = blockIdx.x; ok && u < units; u += gridDim.x) {
-            const int rt = u / splits, sp = u - (u / splits) * splits;
+            int local;
+            const PassParams &Q = unit_params<BAT>(P0, plist, unit_start, count, u, local);
+            if (BAT && pass_skipped(Q)) continue;
+            const int splits = Q.ft_splits, tps = Q.ft_tps, ctiles = Q.ft_ctiles, rtiles = Q.ft_rtiles;
+            const int nkb = Q.fkb;
+            const int rt = local / splits, sp = local - (local / splits) * splits;
             const int ct0 = sp * tps, ct1 = min(ctiles, ct0 + tps);
             for (int ct = ct0; ok && ct < ct1; ++ct) {
                 for (int kb = 0; kb < nkb; ++kb, ++it) {
@@ -252,12 +284,12 @@ __global__ void __launch_bounds__(FT_THREADS, 1)
 #pragma unroll
                         for (int p = 0; p < NP; ++p)
                             bulk_g2s(dst + p * FT_PIECE_BYTES,
-                                     P.fx + ((size_t)(p * rtiles + rt) * nkb + kb) * FT_PIECE_ELEMS,
+                                     Q.fx + ((size_t)(p * rtiles + rt) * nkb + kb) * FT_PIECE_ELEMS,
                                      FT_PIECE_BYTES, FULL + 8u * s);
 #pragma unroll
                         for (int p = 0; p < NP; ++p)
                             bulk_g2s(dst + (NP + p) * FT_PIECE_BYTES,
-                                     P.fy + ((size_t)(p * ctiles + ct) * nkb + kb) * FT_PIECE_ELEMS,
+                                     Q.fy + ((size_t)(p * ctiles + ct) * nkb + kb) * FT_PIECE_ELEMS,
                                      FT_PIECE_BYTES, FULL + 8u * s);
 #pragma unroll
                         for (int s2 = 0; s2 < NS; ++s2)
@@ -282,7 +314,11 @@ __global__ void __launch_bounds__(FT_THREADS, 1)
         int it = 0, tc = 0;
         bool ok = true;
         for (int u = blockIdx.x; ok && u < units; u += gridDim.x) {
-            const int sp = u - (u / splits) * splits;
+            int local;
+            const PassParams &Q = unit_params<BAT>(P0, plist, unit_start, count, u, local);
+            if (BAT && pass_skipped(Q)) continue;
+            const int splits = Q.ft_splits, tps = Q.ft_tps, ctiles = Q.ft_ctiles, nkb = Q.fkb;
+            const int sp = local - (local / splits) * splits;
             const int ct0 = sp * tps, ct1 = min(ctiles, ct0 + tps);
             for (int ct = ct0; ok && ct < ct1; ++ct, ++tc) {
                 const int b = tc & 1;
@@ -329,16 +365,23 @@ __global__ void __launch_bounds__(FT_THREADS, 1)
         const int rloc = quad * 32 + lane;          // row within the tile
         float *gw = colterm + (size_t)(warp - 2) * 2 * FT_N;   // this warp's column terms
         float *yw = gw + FT_N;
-        const double a2 = alpha * LOG2E;
-        const double cb = P.colpot_unit ? LOG2E : beta * LOG2E;
-        const float k2 = (float)(-2.0 * a2);        // log2 exponent per unit of <x, y>
         int tc = 0;
         bool ok = true;
         for (int u = blockIdx.x; ok && u < units; u += gridDim.x) {
-            const int rt = u / splits, sp = u - (u / splits) * splits;
+            int local;
+            const PassParams &Q = unit_params<BAT>(P0, plist, unit_start, count, u, local);
+            if (BAT && pass_skipped(Q)) continue;
+            double alpha = 0.0, beta = 0.0;
+            if (ACC == ACC_LSE) resolve_coefs(Q, alpha, beta);
+            const double a2 = alpha * LOG2E;
+            const double cb = Q.colpot_unit ? LOG2E : beta * LOG2E;
+            const float k2 = (float)(-2.0 * a2);    // log2 exponent per unit of <x, y>
+            const int splits = Q.ft_splits, tps = Q.ft_tps, ctiles = Q.ft_ctiles;
+            const int rt = local / splits, sp = local - (local / splits) * splits;
             const int ct0 = sp * tps, ct1 = min(ctiles, ct0 + tps);
+            const int n = Q.n, m = Q.m;
             const int row = rt * FT_M + rloc;
-            const float xnf = (MOM && row < P.n) ? (float)P.xn[row] : 0.f;
+            const float xnf = (MOM && row < n) ? (float)Q.xn[row] : 0.f;
             float M = (ACC == ACC_MIN) ? INFINITY : ((ACC == ACC_MAX) ? -INFINITY : -1e30f);
             KSum S;
             S.s = 0.f;
@@ -354,11 +397,11 @@ __global__ void __launch_bounds__(FT_THREADS, 1)
                     const int jj = i * 32 + lane;
                     const int j = ct * FT_N + jj;
                     float g, yv = 0.f;
-                    if (j < P.m) {
-                        const double pot = P.colpot ? P.colpot[j] : 0.0;
-                        const double ynj = P.yn[j];
+                    if (j < m) {
+                        const double pot = Q.colpot ? Q.colpot[j] : 0.0;
+                        const double ynj = Q.yn[j];
                         if (ACC == ACC_LSE) g = (float)(((cb == 0.0) ? 0.0 : cb * pot) + a2 * ynj);
-                        else if (ACC == ACC_MIN) g = (float)(ynj + P.minmax_scale * pot);
+                        else if (ACC == ACC_MIN) g = (float)(ynj + Q.minmax_scale * pot);
                         else g = (float)ynj;
                         yv = (float)ynj;
                     } else {
@@ -414,14 +457,14 @@ __global__ void __launch_bounds__(FT_THREADS, 1)
                 if (lane == 0) mbar_arrive(ACCE + 8u * b);   // accumulator b may be overwritten
             }
             if (!ok) break;
-            if (row < P.n) {
-                double *pp = P.part + ((size_t)sp * P.n + row) * 3;
+            if (row < n) {
+                double *pp = Q.part + ((size_t)sp * n + row) * 3;
                 if (ACC == ACC_LSE) {
                     pp[0] = (double)M;
                     pp[1] = (double)S.s - (double)S.c;
                     if (MOM) pp[2] = (double)MO;
                 } else {
-                    pp[0] = (double)M + P.xn[row];
+                    pp[0] = (double)M + Q.xn[row];
                 }
             }
         }
@@ -433,17 +476,47 @@ __global__ void __launch_bounds__(FT_THREADS, 1)
     if (warp == 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(FT_TMEM_COLS)
                      : "memory");
-    if (threadIdx.x == 0 && *abort_flag && ctl) {
-        ctl->error = CULAMP_ERR_DEVICE_TIMEOUT;
-        ctl->stop = 1;
+    if (threadIdx.x == 0 && *abort_flag) {
+        if (BAT) {
+            if (batch_err) atomicExch(batch_err, CULAMP_ERR_DEVICE_TIMEOUT);
+        } else if (P0.ctl) {
+            P0.ctl->error = CULAMP_ERR_DEVICE_TIMEOUT;
+            P0.ctl->stop = 1;
+        }
     }
 }
 
 // Merge the column-slice partials of each row and run the pass epilogue.
-template <int ACC, bool MOM>
-__global__ void __launch_bounds__(TPB) feat_merge_kernel(PassParams P) {
+// BAT: blocks of many instances (block_start[i] .. block_start[i+1]-1 are the
+// row blocks of instance i, P.nrb of them).
+template <int ACC, bool MOM, bool BAT>
+__global__ void __launch_bounds__(TPB)
+    feat_merge_kernel(const __grid_constant__ PassParams P0, const PassParams *plist,
+                      const int *block_start, int count) {
     __shared__ double red[4 * (TPB / 32)];
     __shared__ int s_last;
+    __shared__ int s_blk[2];
+    __shared__ __align__(16) PassParams sP;
+    if constexpr (BAT) {
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = count - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (block_start[mid] <= (int)blockIdx.x) lo = mid;
+                else hi = mid - 1;
+            }
+            s_blk[0] = (int)blockIdx.x - block_start[lo];
+            s_blk[1] = lo;
+        }
+        __syncthreads();
+        const int *src = reinterpret_cast<const int *>(plist + s_blk[1]);
+        int *dst = reinterpret_cast<int *>(&sP);
+        for (int k = threadIdx.x; k < (int)(sizeof(PassParams) / sizeof(int)); k += TPB) dst[k] = src[k];
+        __syncthreads();
+    }
+    const PassParams &P = *(BAT ? &sP : &P0);
+    const int rb = BAT ? s_blk[0] : (int)blockIdx.x;
+    const int nrb = BAT ? P.nrb : (int)gridDim.x;
     Ctl *ctl = P.ctl;
     if (ctl) {
         if (ctl->stop) return;
@@ -452,7 +525,6 @@ __global__ void __launch_bounds__(TPB) feat_merge_kernel(PassParams P) {
     }
     double alpha = 0.0, beta = 0.0;
     if (ACC == ACC_LSE) resolve_coefs(P, alpha, beta);
-    const int rb = blockIdx.x;
     const int row_base = rb * (TPB * RPT);
     double Mv[RPT], Sv[RPT], MOMv[RPT], Hv[RPT];
 #pragma unroll
@@ -473,7 +545,7 @@ __global__ void __launch_bounds__(TPB) feat_merge_kernel(PassParams P) {
         MOMv[r] = MO;
         Hv[r] = (ACC == ACC_LSE && row < P.n) ? alpha * LOG2E * P.xn[row] : 0.0;
     }
-    row_epilogue<ACC, RPT>(P, rb, row_base, beta, Mv, Sv, MOMv, Hv, red, s_last, gridDim.x);
+    row_epilogue<ACC, RPT>(P, rb, row_base, beta, Mv, Sv, MOMv, Hv, red, s_last, nrb);
 }
 
 // Round to the nearest bf16 value, ties to even, on the FP64 bit pattern (keep
@@ -537,9 +609,11 @@ __global__ void feat_norm_kernel(double *out, const double *X, int n, int d) {
     if (lane == 0) out[row] = s;
 }
 
-template <int NP, int ACC, bool MOM>
-cudaError_t launch_ft(const PassParams &P, const culamp_host::FeatShape &fs, cudaStream_t st) {
-    auto kern = feat_reduce_kernel<NP, ACC, MOM>;
+template <int NP, int ACC, bool MOM, bool BAT>
+cudaError_t launch_ft(const PassParams &P, const PassParams *plist, const int *unit_start,
+                      const int *block_start, int count, int total_units, int merge_blocks,
+                      int grid, int *batch_err, cudaStream_t st) {
+    auto kern = feat_reduce_kernel<NP, ACC, MOM, BAT>;
     constexpr size_t smem = ft_smem_bytes<NP>();
     static bool attr_set = false;   // per instantiation; same value on every device
     if (!attr_set) {
@@ -547,21 +621,28 @@ cudaError_t launch_ft(const PassParams &P, const culamp_host::FeatShape &fs, cud
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    kern<<<fs.grid, FT_THREADS, smem, st>>>(P, fs.rtiles, fs.ctiles, fs.splits, fs.tps);
+    kern<<<grid, FT_THREADS, smem, st>>>(P, plist, unit_start, count, total_units, batch_err);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    feat_merge_kernel<ACC, MOM><<<fs.merge_rb, TPB, 0, st>>>(P);
+    feat_merge_kernel<ACC, MOM, BAT><<<merge_blocks, TPB, 0, st>>>(P, plist, block_start, count);
     return cudaGetLastError();
 }
 
-template <int NP>
-cudaError_t launch_ft_acc(const PassParams &P, int acc, const culamp_host::FeatShape &fs, cudaStream_t st) {
-    if (acc == ACC_LSE) {
-        if (P.want_moment) return launch_ft<NP, ACC_LSE, true>(P, fs, st);
-        return launch_ft<NP, ACC_LSE, false>(P, fs, st);
+template <bool BAT>
+cudaError_t launch_ft_any(int np, int acc, bool mom, const PassParams &P, const PassParams *plist,
+                          const int *unit_start, const int *block_start, int count, int total_units,
+                          int merge_blocks, int grid, int *batch_err, cudaStream_t st) {
+#define CULAMP_FT(NP_, ACC_, MOM_) \
+    launch_ft<NP_, ACC_, MOM_, BAT>(P, plist, unit_start, block_start, count, total_units, merge_blocks, grid, batch_err, st)
+    if (np == 2) {
+        if (acc == ACC_LSE) return mom ? CULAMP_FT(2, ACC_LSE, true) : CULAMP_FT(2, ACC_LSE, false);
+        if (acc == ACC_MAX) return CULAMP_FT(2, ACC_MAX, false);
+        return CULAMP_FT(2, ACC_MIN, false);
     }
-    if (acc == ACC_MAX) return launch_ft<NP, ACC_MAX, false>(P, fs, st);
-    return launch_ft<NP, ACC_MIN, false>(P, fs, st);
+    if (acc == ACC_LSE) return mom ? CULAMP_FT(3, ACC_LSE, true) : CULAMP_FT(3, ACC_LSE, false);
+    if (acc == ACC_MAX) return CULAMP_FT(3, ACC_MAX, false);
+    return CULAMP_FT(3, ACC_MIN, false);
+#undef CULAMP_FT
 }
 
 }  // namespace
@@ -624,13 +705,34 @@ cudaError_t launch_feat_pass(PassParams P, int acc, Scratch &scr, int sm_count, 
     if (scr.part.bytes < fs.part_bytes || scr.tickets.bytes < (size_t)(fs.merge_rb + 1) * sizeof(unsigned) ||
         scr.blk.bytes < (size_t)fs.merge_rb * 4 * sizeof(double))
         return cudaErrorInvalidValue;
-    P.splits = fs.splits;
-    P.cols_per_split = fs.tps * FT_N;
+    set_feat_geometry(P, fs);
     P.part = scr.part.as<double>();
     P.rb_ticket = scr.tickets.as<unsigned>();
     P.grid_ticket = scr.tickets.as<unsigned>() + fs.merge_rb;
     P.blk = scr.blk.as<double>();
-    return P.fpieces == 2 ? launch_ft_acc<2>(P, acc, fs, st) : launch_ft_acc<3>(P, acc, fs, st);
+    return launch_ft_any<false>(P.fpieces, acc, P.want_moment != 0, P, nullptr, nullptr, nullptr, 1,
+                                fs.units, fs.merge_rb, fs.grid, nullptr, st);
+}
+
+void set_feat_geometry(PassParams &P, const FeatShape &fs) {
+    P.splits = fs.splits;
+    P.cols_per_split = fs.tps * FT_N;
+    P.nrb = fs.merge_rb;
+    P.ft_rtiles = fs.rtiles;
+    P.ft_ctiles = fs.ctiles;
+    P.ft_splits = fs.splits;
+    P.ft_tps = fs.tps;
+}
+
+cudaError_t launch_feat_batched(int np, int acc, bool mom, const PassParams *plist, const int *unit_start,
+                                const int *block_start, int count, int total_units, int merge_blocks,
+                                int sm_count, int *batch_err, cudaStream_t st) {
+    if (count < 1 || total_units < 1) return cudaSuccess;
+    PassParams dummy;
+    memset(&dummy, 0, sizeof(dummy));
+    const int grid = total_units < sm_count ? total_units : sm_count;
+    return launch_ft_any<true>(np, acc, mom, dummy, plist, unit_start, block_start, count, total_units,
+                               merge_blocks, grid, batch_err, st);
 }
 
 }  // namespace culamp_host

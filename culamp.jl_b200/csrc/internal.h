@@ -74,6 +74,11 @@ LaunchShape pass_shape(int n, int m, int d, int acc, int sm_count, bool mom = fa
 cudaError_t launch_pass(PassParams P, int pmode, int acc, const LaunchShape &sh, Scratch &scr,
                         cudaStream_t st);
 
+// The same with explicit scratch (partials, row-block tickets + grid ticket,
+// block scalars) sized by the caller for `sh`.
+cudaError_t launch_pass_at(PassParams P, int pmode, int acc, const LaunchShape &sh, double *part,
+                           unsigned *tickets, double *blk, cudaStream_t st);
+
 int pmode_of(double p);   // P_L1 / P_SQ / P_INF / P_GEN
 
 // ---- feature-cost path (feature.cu): p = 2, d >= FEAT_MIN_D, tensor cores
@@ -95,6 +100,18 @@ cudaError_t feat_prepare(uint16_t *pieces, double *norms, const double *X, int n
                          cudaStream_t st);
 // Reduction on the tensor cores + merge / epilogue; P.fx .. P.fpieces set.
 cudaError_t launch_feat_pass(PassParams P, int acc, Scratch &scr, int sm_count, cudaStream_t st);
+// Work-unit geometry of a feature pass (splits, tiles, merge row blocks) into P.
+void set_feat_geometry(PassParams &P, const FeatShape &fs);
+// One batched feature pass over `count` instances (device parameter list,
+// unit and merge-block prefix tables with count + 1 entries).
+cudaError_t launch_feat_batched(int np, int acc, bool mom, const PassParams *plist, const int *unit_start,
+                                const int *block_start, int count, int total_units, int merge_blocks,
+                                int sm_count, int *batch_err, cudaStream_t st);
+// One batched pair pass (pair_pass_kernel<..., BAT = true>) over `count`
+// instances of dimension d (d <= 3 packed, else generic), RPT rows per thread.
+cudaError_t launch_pass_batched(const PassParams *plist, const int *block_start, int count,
+                                int total_blocks, size_t smem, int pmode, int d, int acc, bool mom,
+                                bool fixed_ref, cudaStream_t st);
 
 }  // namespace culamp_host
 
@@ -108,6 +125,8 @@ struct culamp_handle_s {
     culamp_host::DevBuf tmpA, tmpB;    // pass-level temporaries
     struct Solver;                     // solver workspaces and cached graphs
     Solver *solver = nullptr;
+    struct Batch;                      // batched-solve workspace, tuned shapes, graph
+    Batch *batch = nullptr;
 };
 
 int culamp_set_error(culamp_handle h, int code, const char *fmt, ...);

@@ -57,6 +57,25 @@ class CStats(C.Structure):
                 ("stopped", C.c_int32), ("status", C.c_int32)]
 
 
+class CInstance(C.Structure):
+    _fields_ = [("x", C.c_void_p), ("y", C.c_void_p), ("r", C.c_void_p), ("c", C.c_void_p),
+                ("phi", C.c_void_p), ("psi", C.c_void_p), ("n", C.c_int64), ("m", C.c_int64),
+                ("d", C.c_int32), ("reserved", C.c_int32)]
+
+
+class CBatchStats(C.Structure):
+    _fields_ = [("iterations", C.c_int64), ("num_iter", C.c_int64), ("residual", C.c_double),
+                ("objective", C.c_double), ("winf", C.c_double), ("stopped", C.c_int32),
+                ("status", C.c_int32)]
+
+
+class CBatchInfo(C.Structure):
+    _fields_ = [("elapsed_ms", C.c_double), ("tune_ms", C.c_double),
+                ("target_ctas_per_sm", C.c_int32), ("feat_tiles_per_unit", C.c_int32),
+                ("unroll", C.c_int32), ("launches_per_iteration", C.c_int32),
+                ("phases", C.c_int32), ("reserved", C.c_int32)]
+
+
 _VP = C.c_void_p
 _D = C.c_double
 _I64 = C.c_int64
@@ -103,6 +122,8 @@ SIGNATURES = {
                                     _VP]),
     "culamp_lse_rows_sk_noalloc": (C.c_int, [_VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, _D, _D, _D,
                                              _VP]),
+    "culamp_batched_sinkhorn": (C.c_int, [_VP, C.POINTER(CInstance), _I32, C.POINTER(CArgs), _I64, _D,
+                                          _U32, C.POINTER(CBatchStats), C.POINTER(CBatchInfo), _VP]),
     "culamp_marginal_error_fp64": (C.c_int, [_VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, _VP, _VP,
                                              _D, _D, _D, C.POINTER(_D), C.POINTER(_D), _VP]),
 }

@@ -407,3 +407,57 @@ def _np(a):
     if _is_torch(a):
         return a.detach().cpu().numpy()
     return a
+
+
+# ------------------------------------------------------------------ batched solves
+
+@dataclass
+class BatchResult:
+    results: list            # one SolveResult per instance (phi, psi on the device)
+    elapsed_ms: float        # device time of the solve loop
+    tune_ms: float           # device time spent timing shape candidates (0 when cached)
+    target_ctas_per_sm: int
+    feat_tiles_per_unit: int
+    unroll: int
+    launches_per_iteration: int
+    phases: int
+
+
+def solve_batched_sinkhorn(instances, args: EOTArgs, frequency: int = 100, p: float = 2.0,
+                           flags: int = 0, handle: Handle | None = None) -> BatchResult:
+    """Many independent kernel Sinkhorn problems of uneven n, m, d in one solve
+    (culamp_batched_sinkhorn). `instances`: sequence of (x, y, r, c) float64
+    CUDA tensors on one device. Each result equals what solve_sinkhorn gives for
+    that instance alone (same iterations and stopping rule)."""
+    import torch
+    inst = list(instances)
+    if not inst:
+        raise ValueError("empty batch")
+    dev = inst[0][0].device
+    h = handle or get_handle(dev.index)
+    arr = (_lib.CInstance * len(inst))()
+    outs = []
+    for k, (x, y, r, c) in enumerate(inst):
+        n, d = _points(x)
+        m, d2 = _points(y)
+        if d != d2:
+            raise ValueError(f"instance {k}: x and y dimensions differ")
+        phi = torch.empty(n, dtype=torch.float64, device=dev)
+        psi = torch.empty(m, dtype=torch.float64, device=dev)
+        e = arr[k]
+        e.x, e.y = _dev(x, "x", n, 2), _dev(y, "y", m, 2)
+        e.r, e.c = _dev(r, "r", n, 1), _dev(c, "c", m, 1)
+        e.phi, e.psi = phi.data_ptr(), psi.data_ptr()
+        e.n, e.m, e.d = n, m, d
+        outs.append((phi, psi))
+    stats = (_lib.CBatchStats * len(inst))()
+    info = _lib.CBatchInfo()
+    a = args.to_c()
+    st = h._lib.culamp_batched_sinkhorn(h.ptr, arr, len(inst), C.byref(a), int(frequency), float(p),
+                                        int(flags), stats, C.byref(info), _stream())
+    h.check(st, "culamp_batched_sinkhorn")
+    res = [SolveResult(phi, psi, s.residual, s.objective, int(s.iterations), int(s.num_iter), s.winf,
+                       math.nan, int(s.stopped)) for (phi, psi), s in zip(outs, stats)]
+    return BatchResult(res, info.elapsed_ms, info.tune_ms, info.target_ctas_per_sm,
+                       info.feat_tiles_per_unit, info.unroll, info.launches_per_iteration,
+                       info.phases)

@@ -206,6 +206,58 @@ int culamp_annealed_sinkhorn(culamp_handle h, const double *x, const double *y, 
                              uint32_t flags, double *phi, double *psi, culamp_stats *stats,
                              culamp_log_row *log, int64_t log_cap, void *stream);
 
+/* ---------------------------------------------------------------- batched solves */
+/* Many independent Sinkhorn problems of uneven n, m and d solved together. No
+ * counterpart in the reference (its drivers solve one problem per call); each
+ * instance follows sinkhorn_color_transfer (SinkhornKernel.jl:477-559) exactly as
+ * culamp_sinkhorn would -- same iterations, checks and stopping rule -- with its
+ * own control state. Every half-step of every class of instance (d <= 3, other
+ * d on the FP64 pair loops, d >= 32 with p = 2 on the tensor cores) is one
+ * launch over all instances, and the loop over iterations runs in CUDA graphs
+ * with a device-side loop condition: one graph launch per phase, a phase ending
+ * when the work of the instances still running has halved, after which the
+ * survivors are re-planned with finer column splits. Tile shapes are chosen by
+ * timing candidates on the batch itself (cached per batch signature). */
+typedef struct culamp_instance {
+    const double *x;      /* n x d points (device)                                     */
+    const double *y;      /* m x d points (device)                                     */
+    const double *r;      /* n row marginal (device)                                   */
+    const double *c;      /* m column marginal (device)                                */
+    double *phi;          /* n output potential (device)                               */
+    double *psi;          /* m output potential (device)                               */
+    int64_t n, m;
+    int32_t d;
+    int32_t reserved;
+} culamp_instance;
+
+typedef struct culamp_batch_stats {
+    int64_t iterations;   /* as culamp_stats.iterations                                */
+    int64_t num_iter;
+    double residual;      /* final L1 row residual (FP64 sums)                         */
+    double objective;     /* final transport cost                                      */
+    double winf;
+    int32_t stopped;      /* 1 tolerance, 2 itermax, 3 tmax                            */
+    int32_t status;
+} culamp_batch_stats;
+
+typedef struct culamp_batch_info {
+    double elapsed_ms;    /* device time of the solve loop (one graph launch)          */
+    double tune_ms;       /* device time spent timing shape candidates (0 when cached) */
+    int32_t target_ctas_per_sm;   /* chosen pair-pass shape: CTAs per SM over the batch */
+    int32_t feat_tiles_per_unit;  /* chosen feature-pass work-unit size (column tiles)  */
+    int32_t unroll;       /* iterations per graph body (last phase)                    */
+    int32_t launches_per_iteration;
+    int32_t phases;       /* graph launches: the loop re-plans when the running work halves */
+    int32_t reserved;
+} culamp_batch_info;
+
+/* p = 1 or 2 (p = Inf follows the reference and iterates on the squared cost).
+ * flags: CULAMP_FLAG_FEAT_X6 / CULAMP_FLAG_FEAT_FP64 / CULAMP_FLAG_NO_GRAPH.
+ * stats: count entries (may be NULL); info may be NULL. */
+int culamp_batched_sinkhorn(culamp_handle h, const culamp_instance *inst, int32_t count,
+                            const culamp_args *args, int64_t frequency, double p, uint32_t flags,
+                            culamp_batch_stats *stats, culamp_batch_info *info, void *stream);
+
 /* Host-buffer variants: same arguments with host pointers; copies in, solves and
  * copies out (the end-to-end path a Julia Array caller uses). */
 int culamp_sinkhorn_host(culamp_handle h, const double *x, const double *y, int64_t n,
