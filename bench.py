@@ -415,6 +415,9 @@ def main():
     # kernel launches per solve: W_inf pass + 3 per iteration (row, column, gated check)
     line["gpu_launches"] = args.steps * (1 + 3 * it_med + 3)
 
+    if world > 1 and not args.no_extras:
+        # every rank takes part (collectives); rank 0 reports
+        line["extras"] = {"sharded_65536": sharded_extra(cb, D, torch, dev, dist, world, rank)}
     if rank == 0 and world == 1 and not args.no_extras:
         line["extras"] = extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_med, value)
         line["extras"]["batched_512"] = batched_extra(cb, D, torch, np, dev, dfma, ex2)
@@ -465,6 +468,35 @@ def extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_chosen, chosen_ms):
                             "pass_gpair_s": 65536.0 ** 2 / (ms5 * 1e-3) / 1e9}
     ex["features_16384_d256"] = feature_extra(cb, D, torch, dev)
     return ex
+
+
+def sharded_extra(cb, D, torch, dev, dist, world, rank):
+    """Row-sharded Sinkhorn (strong scaling): the 65536-point RGB instance
+    (eta_p = 1e-3, to 1e-6 L1, check every 25 iterations) with its rows split
+    over the ranks, one block per GPU; per iteration one all_gather of the
+    65536 column partials. Device time (CUDA events) of the solve, max over
+    ranks."""
+    from culamp_b200.sharded import shard_rows, sharded_sinkhorn
+    x5, y5, r5, c5 = D.rgb_instance(65536, 65536)
+    s, e = shard_rows(x5.shape[0], world, rank)
+    X, R = (torch.as_tensor(v[s:e].copy(), device=dev) for v in (x5, r5))
+    Y, C5 = (torch.as_tensor(v, device=dev) for v in (y5, c5))
+    a = cb.EOTArgs(eta_p=ETA, epsilon=EPS, itermax=20000, tmax=60.0, verbose=False)
+    sharded_sinkhorn([X], [R], Y, C5, a.copy(itermax=5), 25, P)        # warm-up
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    res = sharded_sinkhorn([X], [R], Y, C5, a, 25, P)
+    e1.record()
+    e1.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1)], device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return {"ranks": world, "rows_per_rank": e - s, "ms": float(t.item()), "iterations": res.iterations,
+            "reached_tol": res.stopped == 1, "residual": res.residual, "objective": res.objective,
+            "scaling": "strong", "timing": "CUDA events around the solve, max over ranks"}
 
 
 def batched_extra(cb, D, torch, np, dev, dfma, ex2, count=512, sample=24):

@@ -383,6 +383,18 @@ extern "C" int culamp_min_reduce(culamp_handle h, double *out, const double *x, 
     return run_pass(h, P, pmode_of(p), ACC_MIN, (cudaStream_t)stream);
 }
 
+extern "C" int culamp_lse_combine(culamp_handle h, double *psi, const double *parts, int32_t shards,
+                                  int64_t m, void *stream) {
+    if (!h) return CULAMP_ERR_INVALID_ARG;
+    if (!psi || !parts || shards < 1 || m < 1)
+        return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "bad lse_combine arguments");
+    cudaSetDevice(h->device);
+    lse_combine_kernel<<<(unsigned)((m + 255) / 256), 256, 0, (cudaStream_t)stream>>>(psi, parts, shards, m);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return culamp_set_error(h, CULAMP_ERR_CUDA, "lse_combine: %s", cudaGetErrorString(e));
+    return CULAMP_OK;
+}
+
 extern "C" int culamp_theta_update(culamp_handle h, double *theta, const double *theta0,
                                    const double *residual, const double *c,
                                    const double *eta_mu_i, double eta_mu, int32_t adjust,

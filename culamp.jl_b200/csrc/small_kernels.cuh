@@ -15,6 +15,20 @@ static __global__ void log_minus_kernel(double *out, const double *marg, const d
     if (i < n) out[i] = log(marg[i]) - logz[i];
 }
 
+// Column potentials of a row-sharded Sinkhorn from the shards' column passes:
+// shard g computed out_g,j = log c_j - LSE_{i in g}(...); the full column LSE
+// is the log-sum-exp over shards, so psi_j = -log sum_g exp(-out_g,j) (FP64,
+// max-shifted). parts: G rows of m.
+static __global__ void lse_combine_kernel(double *psi, const double *parts, int G, long long m) {
+    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= m) return;
+    double mx = -INFINITY;
+    for (int g = 0; g < G; ++g) mx = fmax(mx, -parts[(size_t)g * m + j]);
+    double s = 0.0;
+    for (int g = 0; g < G; ++g) s += exp(-parts[(size_t)g * m + j] - mx);
+    psi[j] = -(mx + log(s));
+}
+
 // update_theta_residual (MirrorProx.jl:159-180), elementwise.
 static __global__ void theta_update_kernel(double *theta, const double *theta0, const double *residual,
                                     const double *c, const double *eta_mu_i, double eta_mu,

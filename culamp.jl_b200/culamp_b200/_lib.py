@@ -122,6 +122,7 @@ SIGNATURES = {
                                     _VP]),
     "culamp_lse_rows_sk_noalloc": (C.c_int, [_VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, _D, _D, _D,
                                              _VP]),
+    "culamp_lse_combine": (C.c_int, [_VP, _VP, _VP, _I32, _I64, _VP]),
     "culamp_batched_sinkhorn": (C.c_int, [_VP, C.POINTER(CInstance), _I32, C.POINTER(CArgs), _I64, _D,
                                           _U32, C.POINTER(CBatchStats), C.POINTER(CBatchInfo), _VP]),
     "culamp_marginal_error_fp64": (C.c_int, [_VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, _VP, _VP,

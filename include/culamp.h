@@ -206,6 +206,16 @@ int culamp_annealed_sinkhorn(culamp_handle h, const double *x, const double *y, 
                              uint32_t flags, double *phi, double *psi, culamp_stats *stats,
                              culamp_log_row *log, int64_t log_cap, void *stream);
 
+/* Row-sharded Sinkhorn (several GPUs, or several row blocks on one): shard g's
+ * column pass (culamp_lse_rows_sk over its rows) gives out_g = log c - LSE over
+ * its rows; the column potential is the log-sum-exp over shards,
+ * psi_j = -log sum_g exp(-out_g,j). parts: `shards` device rows of m values
+ * (e.g. an all-gather of the shards' outputs). No counterpart in the reference
+ * (it runs on one GPU); replaces the column LSE of SinkhornKernel.jl:520-523
+ * when the rows are split. */
+int culamp_lse_combine(culamp_handle h, double *psi, const double *parts, int32_t shards, int64_t m,
+                       void *stream);
+
 /* ---------------------------------------------------------------- batched solves */
 /* Many independent Sinkhorn problems of uneven n, m and d solved together. No
  * counterpart in the reference (its drivers solve one problem per call); each
