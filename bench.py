@@ -467,7 +467,34 @@ def extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_chosen, chosen_ms):
                             "pass_ms": ms5, "pass_timing": how5,
                             "pass_gpair_s": 65536.0 ** 2 / (ms5 * 1e-3) / 1e9}
     ex["features_16384_d256"] = feature_extra(cb, D, torch, dev)
+    ex["divergence_65536"] = divergence_extra(cb, D, torch, dev, X5, Y5, R5, C5, s5.winf)
     return ex
+
+
+def divergence_extra(cb, D, torch, dev, X, Y, R, Cc, winf_xy):
+    """Sinkhorn divergence S = OT(a,b) - OT(a,a)/2 - OT(b,b)/2 of the 65536-point
+    RGB clouds at eps = eta_p * W_inf(x, y) (absolute, shared by the three
+    solves, each to 1e-6 L1), then dS/dx, dS/dy by the adjoint pass (six passes
+    over n*m pairs, P_ij recomputed, nothing n x m stored) and dS/da, dS/db
+    from the potentials. Device time with CUDA events."""
+    from culamp_b200.divergence import divergence_grads, sinkhorn_divergence
+    eps = ETA * winf_xy
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record()
+    parts = sinkhorn_divergence(X, Y, R, Cc, eps, P, tol=1e-6, frequency=25)
+    e[1].record()
+    gx, gy, ga, gb = divergence_grads(X, Y, parts, P)
+    e[2].record()
+    e[2].synchronize()
+    grad_ms = e[1].elapsed_time(e[2])
+    pairs = 6.0 * X.shape[0] * Y.shape[0]
+    return {"eps": eps, "value": parts.value, "forward_ms": e[0].elapsed_time(e[1]),
+            "iterations": [parts.xy.iterations, parts.xx.iterations, parts.yy.iterations],
+            "residuals": [parts.xy.residual, parts.xx.residual, parts.yy.residual],
+            "adjoint_ms": grad_ms, "adjoint_gpair_s": pairs / (grad_ms * 1e-3) / 1e9,
+            "grad_finite": bool(torch.isfinite(gx).all() and torch.isfinite(gy).all()),
+            "checks": "adjoint vs FP64 envelope gradient and vs central differences: "
+                      "tests/test_gpu_divergence.py"}
 
 
 def sharded_extra(cb, D, torch, dev, dist, world, rank):
