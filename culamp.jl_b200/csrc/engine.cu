@@ -19,9 +19,13 @@ int pmode_of(double p) {
 LaunchShape pass_shape(int n, int m, int d, int acc, int sm_count, bool mom) {
     LaunchShape s{};
     const bool packed = d >= 1 && d <= MAXD_PACKED;
-    // 8 rows per thread amortise each broadcast column over more pairs; used
-    // when there are enough row blocks to fill the GPU with few column splits.
-    s.R = (acc == ACC_LSE && packed && !mom && n >= 16384) ? RPT_BIG : RPT;
+    const int sms = sm_count > 0 ? sm_count : 148;
+    // More rows per thread amortise each broadcast column over more pairs;
+    // used when there are enough row blocks to fill the GPU with few column
+    // splits. Measured (row pass, d = 3): 4 rows beat 8 by 16 % at 16384^2
+    // (4 CTAs per SM instead of 3), 8 beat 4 by 4 % at 65536^2.
+    const bool big = acc == ACC_LSE && packed && !mom;
+    s.R = (big && n >= 32768) ? RPT_BIG : ((big && n >= 16384) ? RPT_MID : RPT);
     const int rows = TPB * s.R;
     s.rb = (n + rows - 1) / rows;
     if (s.rb < 1) s.rb = 1;
@@ -29,22 +33,35 @@ LaunchShape pass_shape(int n, int m, int d, int acc, int sm_count, bool mom) {
     // (64 / 128 columns) cost more in per-CTA overhead and merging than the
     // extra CTAs win back
     const int ch = packed ? CHUNK : CHUNK_G;
-    // Aim for ~4 resident CTAs per SM over the whole grid; never split below one tile.
-    const int target = 4 * (sm_count > 0 ? sm_count : 148);
-    int splits = (target + s.rb - 1) / s.rb;
+    // Resident CTAs per SM: the kernels' launch bounds (3 for 8 rows per
+    // thread, 4 otherwise). All CTAs of a pass do the same work, so the pass
+    // takes ceil(CTAs / slots) waves of (columns per split) each: pick the
+    // split count that minimises that, preferring fewer splits on ties (fewer
+    // partials to merge). E.g. 65536^2: 64 row blocks on 444 slots -> 20 splits
+    // (2.9 waves, 95 % of the ideal) rather than 10 (1.4 waves, 72 %).
+    const long long slots = (long long)sms * (s.R > RPT_MID ? 3 : 4);
     const int max_splits = (m + ch - 1) / ch;
-    if (splits > max_splits) splits = max_splits;
-    if (splits < 1) splits = 1;
-    int cps = (m + splits - 1) / splits;
-    cps = ((cps + ch - 1) / ch) * ch;
-    if (cps < ch) cps = ch;
-    splits = (m + cps - 1) / cps;
-    if (splits < 1) splits = 1;
-    s.splits = splits;
-    s.cols_per_split = cps;
+    int best_splits = 1, best_cps = ((m + ch - 1) / ch) * ch;
+    double best_cost = 1e300;
+    for (int sp = 1; sp <= max_splits; ++sp) {
+        int cps = (m + sp - 1) / sp;
+        cps = ((cps + ch - 1) / ch) * ch;
+        const int spr = (m + cps - 1) / cps;
+        if (spr != sp) continue;                  // same shape as a smaller count
+        const long long ctas = (long long)s.rb * spr;
+        const long long waves = (ctas + slots - 1) / slots;
+        const double cost = (double)waves * (double)cps * (1.0 + 0.002 * spr);
+        if (cost < best_cost * (1.0 - 1e-9)) {
+            best_cost = cost;
+            best_splits = spr;
+            best_cps = cps;
+        }
+    }
+    s.splits = best_splits;
+    s.cols_per_split = best_cps;
     s.smem = (size_t)(packed ? CHUNK * 4 : CHUNK_G * (d + 1)) * sizeof(double);
-    s.part_bytes = splits > 1 ? (size_t)splits * (size_t)n * 3 * sizeof(double) : 0;
-    s.sms = sm_count > 0 ? sm_count : 148;
+    s.part_bytes = s.splits > 1 ? (size_t)s.splits * (size_t)n * 3 * sizeof(double) : 0;
+    s.sms = sms;
     (void)acc;
     return s;
 }
@@ -69,9 +86,11 @@ static cudaError_t launch_v(const PassParams &P, const LaunchShape &sh, cudaStre
         if constexpr (D > 0) {
             if (P.use_ref) {
                 if (sh.R == RPT_BIG) return launch_t<PM, D, ACC, RPT_BIG, false, true>(P, sh, st);
+                if (sh.R == RPT_MID) return launch_t<PM, D, ACC, RPT_MID, false, true>(P, sh, st);
                 return launch_t<PM, D, ACC, RPT, false, true>(P, sh, st);
             }
             if (sh.R == RPT_BIG) return launch_t<PM, D, ACC, RPT_BIG, false>(P, sh, st);
+            if (sh.R == RPT_MID) return launch_t<PM, D, ACC, RPT_MID, false>(P, sh, st);
         }
     }
     return launch_t<PM, D, ACC, RPT, false>(P, sh, st);

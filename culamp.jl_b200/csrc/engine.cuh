@@ -40,7 +40,8 @@ namespace culamp_dev {
 
 constexpr int TPB = 128;          // threads per CTA
 constexpr int RPT = 2;            // output rows per thread, small-problem / generic variants
-constexpr int RPT_BIG = 8;        // output rows per thread, packed log-sum-exp variant
+constexpr int RPT_BIG = 8;        // output rows per thread, packed log-sum-exp, large n
+constexpr int RPT_MID = 4;        // output rows per thread, packed log-sum-exp, mid-size n
 constexpr int ROWS = TPB * RPT;   // output rows per CTA (RPT variant)
 constexpr int CHUNK = 256;        // columns per shared-memory tile (d <= 3)
 constexpr int KC = 4;             // columns per online-max sub-chunk
@@ -779,10 +780,13 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
         int q = 0;
         // few rows per thread (small problems): unroll more columns so each warp
         // has enough independent pairs in flight to cover FP64 / MUFU latency
+        // 16 columns per FP32 chunk sum before the compensated merge: measured
+        // 2.5 % faster than 8 at 65536^2; a 16-term FP32 sum keeps a typical
+        // relative error near 2e-7 of the chunk
         constexpr int FR_UNROLL = (R > RPT) ? 2 : 8;
-        for (; q + 8 <= nc; q += 8) {
+        for (; q + 16 <= nc; q += 16) {
 #pragma unroll FR_UNROLL
-            for (int u = 0; u < 8; ++u) fr_step<PM, D, R>(tile[q + u], xr, a2, P.pexp, K, cs);
+            for (int u = 0; u < 16; ++u) fr_step<PM, D, R>(tile[q + u], xr, a2, P.pexp, K, cs);
 #pragma unroll
             for (int r = 0; r < R; ++r) { kahan_add(S[r], Cc[r], cs[r]); cs[r] = 0.f; }
         }
@@ -1004,7 +1008,7 @@ __device__ __forceinline__ void row_epilogue(const PassParams &P, int rb, int ro
 // and is its local block b - block_start[i] = sp * nrb + rb. Each instance
 // carries its own parameters (plist[i]), scratch, tickets and control block.
 template <int PM, int D, int ACC, int R, bool MOM, bool FR, bool BAT = false>
-__global__ void __launch_bounds__(TPB, (R > RPT) ? 3 : 4)
+__global__ void __launch_bounds__(TPB, (R > RPT_MID) ? 3 : 4)
     pair_pass_kernel(const __grid_constant__ PassParams P0, const PassParams *plist,
                      const int *block_start, int count) {
     extern __shared__ __align__(16) double smem[];
