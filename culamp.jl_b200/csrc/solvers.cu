@@ -8,6 +8,7 @@
 // all live in the passes' device-side "finish" steps, so the host launches the
 // graph once and synchronises once per solve (the reference synchronises after
 // every launch, SinkhornKernel.jl:525 / MirrorProxKernel.jl:1049-1117).
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -64,10 +65,12 @@ enum SolverKind { KIND_SK = 1, KIND_LAMP = 2 };
 // Everything a captured graph bakes into kernel parameters.
 struct GraphKey {
     int kind = 0, n = 0, m = 0, d = 0, pm_iter = 0, pm_resid = 0, unroll = 0, feat = 0;
+    long long freq = 0;   // check cadence the body is aligned to (0: gated checks)
     double p = 0, winf = 0, B = 0, eta_mu = 0;
     long long generation = -1;
     bool operator==(const GraphKey &o) const {
         return kind == o.kind && n == o.n && m == o.m && d == o.d && pm_iter == o.pm_iter && feat == o.feat &&
+               freq == o.freq &&
                pm_resid == o.pm_resid && unroll == o.unroll && generation == o.generation &&
                std::memcmp(&p, &o.p, sizeof(double)) == 0 && std::memcmp(&winf, &o.winf, sizeof(double)) == 0 &&
                std::memcmp(&B, &o.B, sizeof(double)) == 0 && std::memcmp(&eta_mu, &o.eta_mu, sizeof(double)) == 0;
@@ -474,17 +477,31 @@ int sinkhorn_loop(culamp_handle h, int n, int m, int d, double p, double eta, do
     CUDA_TRY(h, cudaMemcpyAsync(S.ctl.ptr, &c, sizeof(Ctl), cudaMemcpyHostToDevice, st));
     set_start_kernel<<<1, 1, 0, st>>>(S.ctl.as<Ctl>());
     SkPlan pl = make_sk_plan(h, n, m, d, p, flags);
-    auto body = [&](cudaStream_t s) -> cudaError_t {
+    // Graph bodies hold whole multiples of `frequency` iterations when the
+    // cadence is short: every body then starts at a check iteration
+    // ((it - 1) % frequency == 0, SinkhornKernel.jl:527), so the residual pass
+    // is recorded only where it runs instead of as a gated launch per iteration.
+    const int base_unroll = pick_unroll((double)n * m * (frequency == 1 ? 3.0 : 2.0));
+    const bool aligned = frequency <= 32;
+    const int unroll = aligned ? (int)frequency * std::max(1, (int)std::lround((double)base_unroll / frequency))
+                               : base_unroll;
+    auto iteration = [&](cudaStream_t s, bool with_check) -> cudaError_t {
         cudaError_t e = launch_pass(pl.k1, pl.pm_iter, ACC_LSE, pl.s_rows, S.scr, s);
         if (e == cudaSuccess) e = launch_pass(pl.k2, pl.pm_iter, ACC_LSE, pl.s_cols, S.scr, s);
-        if (e == cudaSuccess) e = launch_pass(pl.k3, pl.pm_resid, ACC_LSE, pl.s_rows_mom, S.scr, s);
+        if (e == cudaSuccess && with_check) e = launch_pass(pl.k3, pl.pm_resid, ACC_LSE, pl.s_rows_mom, S.scr, s);
         return e;
+    };
+    int body_pos = 0;   // iteration index inside the graph body being recorded
+    auto body = [&](cudaStream_t s) -> cudaError_t {
+        const bool with_check = !aligned || (body_pos % frequency) == 0;
+        body_pos = (body_pos + 1) % unroll;
+        return iteration(s, with_check);
     };
     CUDA_TRY(h, cudaEventRecord(S.ev0, st));
     if (flags & CULAMP_FLAG_NO_GRAPH) {
         // host-driven loop: check the stop flag after every iteration
         for (long long it = 0; it < args->itermax + 2; ++it) {
-            CUDA_TRY(h, body(st));
+            CUDA_TRY(h, iteration(st, true));
             int stop = 0;
             CUDA_TRY(h, cudaMemcpyAsync(&stop, &S.ctl.as<Ctl>()->stop, sizeof(int), cudaMemcpyDeviceToHost, st));
             CUDA_TRY(h, cudaStreamSynchronize(st));
@@ -497,9 +514,11 @@ int sinkhorn_loop(culamp_handle h, int n, int m, int d, double p, double eta, do
         key.pm_iter = pl.pm_iter; key.pm_resid = pl.pm_resid;
         key.p = p;
         key.feat = S.feat_active ? S.feat_np : 0;
-        key.unroll = pick_unroll((double)n * m * (frequency == 1 ? 3.0 : 2.0));
+        key.unroll = unroll;
+        key.freq = aligned ? frequency : 0;
         key.generation = S.generation;
         cudaGraphExec_t ex = nullptr;
+        body_pos = 0;
         int s = get_graph(h, key, body, &ex);
         if (s) return s;
         CUDA_TRY(h, cudaGraphLaunch(ex, st));
@@ -762,7 +781,7 @@ extern "C" int culamp_lamp(culamp_handle h, const double *x, const double *y, in
     CUDA_TRY(h, cudaEventRecord(S.ev0, st));
     if (flags & CULAMP_FLAG_NO_GRAPH) {
         for (long long it = 0; it < args->itermax + 2; ++it) {
-            CUDA_TRY(h, body(st));
+            CUDA_TRY(h, iteration(st, true));
             int stop = 0;
             CUDA_TRY(h, cudaMemcpyAsync(&stop, &S.ctl.as<Ctl>()->stop, sizeof(int), cudaMemcpyDeviceToHost, st));
             CUDA_TRY(h, cudaStreamSynchronize(st));
