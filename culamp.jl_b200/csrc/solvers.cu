@@ -781,7 +781,7 @@ extern "C" int culamp_lamp(culamp_handle h, const double *x, const double *y, in
     CUDA_TRY(h, cudaEventRecord(S.ev0, st));
     if (flags & CULAMP_FLAG_NO_GRAPH) {
         for (long long it = 0; it < args->itermax + 2; ++it) {
-            CUDA_TRY(h, iteration(st, true));
+            CUDA_TRY(h, body(st));
             int stop = 0;
             CUDA_TRY(h, cudaMemcpyAsync(&stop, &S.ctl.as<Ctl>()->stop, sizeof(int), cudaMemcpyDeviceToHost, st));
             CUDA_TRY(h, cudaStreamSynchronize(st));
