@@ -147,7 +147,7 @@ namespace {
 
 using Batch = culamp_handle_s::Batch;
 
-// Pair-pass shape for one batch member: 2 rows per thread, columns split so
+// Pair-pass shape for one batch member: RPT rows per thread, columns split so
 // one CTA handles about `work` pairs.
 LaunchShape batch_pair_shape(int n, int m, int d, double work) {
     LaunchShape s{};
