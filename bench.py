@@ -514,11 +514,14 @@ def extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_chosen, chosen_ms):
         "chosen_over_plain_speedup": (p5.elapsed_ms / s5.elapsed_ms) if p5.stopped == 1 else None,
         "chosen_over_plain_per_iter": (p5.elapsed_ms / max(1, p5.iterations)) /
                                       (s5.elapsed_ms / max(1, s5.iterations))}
+    # LAMP with its full stopping rule (primal-dual gap and marginal error,
+    # MirrorProxKernel.jl:1084-1100): with these uniform marginals the starting
+    # plan already meets the marginal test alone
     bl = cb.EOTArgs(eta_p=ETA, epsilon=EPS, itermax=100_000, tmax=60.0, verbose=False, B=1.1)
-    fl = cb.FLAG_CHECK_ALWAYS | cb.FLAG_MARGINAL_ONLY
-    l5 = cb.solve_lamp(X5, Y5, R5, C5, bl, 25, P, flags=fl)
+    l5 = cb.solve_lamp(X5, Y5, R5, C5, bl, 25, P, flags=cb.FLAG_CHECK_ALWAYS)
+    gap = (l5.log[-1][4] - l5.log[-1][5]) if l5.log else float("nan")
     ex["lamp_65536"] = {"reached_tol": l5.stopped == 1, "ms": l5.elapsed_ms, "iterations": l5.iterations,
-                        "residual": l5.residual}
+                        "residual": l5.residual, "gap": gap, "stop_rule": "gap and marginal"}
     ex["features_16384_d256"] = feature_extra(cb, D, torch, dev)
     ex["divergence_65536"] = divergence_extra(cb, D, torch, dev, X5, Y5, R5, C5, s5.winf)
     return ex
