@@ -432,8 +432,11 @@ def main():
     peak = min(fp64_bound, xu_bound)
     roofline = {"bound": "fp64+xu pipes (not hbm/tensor: operands are L2-resident)",
                 "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gpair/s",
-                "frac": achieved / peak, "traffic": None,
-                "kernel": "pair_pass_kernel<P_SQ,d=2,LSE,R=2,fixed-reference> (fused row LSE)",
+                "frac": achieved / peak,
+                # DRAM bytes per launch (read + write) from one ncu capture of this
+                # kernel in its steady state: profiles/pair_pass_kernel_row_lse_grid4096_steady.md
+                "traffic": 1944576,
+                "kernel": "pair_pass_kernel<P_SQ,d=2,LSE,R=1,fixed-reference> (fused row LSE)",
                 "per_launch_ms": pass_ms, "pairs_per_launch": pairs, "timing": how,
                 "peak_source": "measured in-bench pipe probes (culamp_probe_pipes): "
                                f"DFMA {dfma/1e12:.2f} T/s, ex2 {ex2/1e12:.2f} T/s; "
