@@ -433,8 +433,9 @@ def main():
     roofline = {"bound": "fp64+xu pipes (not hbm/tensor: operands are L2-resident)",
                 "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gpair/s",
                 "frac": achieved / peak,
-                # DRAM bytes per launch (read + write) from one ncu capture of this
-                # kernel in its steady state: profiles/pair_pass_kernel_row_lse_grid4096_steady.md
+                # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
+                # from one ncu capture of this kernel in its steady state
+                # (the --profile-steady target)
                 "traffic": 1944576,
                 "kernel": "pair_pass_kernel<P_SQ,d=2,LSE,R=1,fixed-reference> (fused row LSE)",
                 "per_launch_ms": pass_ms, "pairs_per_launch": pairs, "timing": how,
