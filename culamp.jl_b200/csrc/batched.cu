@@ -171,10 +171,13 @@ LaunchShape batch_pair_shape(int n, int m, int d, double work) {
 }
 
 // Feature-pass shape for one batch member: work units of `tpu` column tiles.
-FeatShape batch_feat_shape(int n, int m, int tpu) {
+FeatShape batch_feat_shape(int n, int m, int tpu, int pieces) {
     FeatShape fs{};
+    fs.ncols = feat_tile_cols(pieces);
     fs.rtiles = (n + 127) / 128;
-    fs.ctiles = (m + 127) / 128;
+    fs.ctiles = (m + fs.ncols - 1) / fs.ncols;
+    fs.rblk = feat_blocks(n);
+    fs.cblk = feat_blocks(m);
     fs.tps = std::min(std::max(tpu, 1), fs.ctiles);
     fs.splits = (fs.ctiles + fs.tps - 1) / fs.tps;
     fs.units = fs.rtiles * fs.splits;
@@ -291,7 +294,7 @@ Plan make_plan(const Ctx &X, int tpsm, int tpu, int sms, const std::vector<int> 
                     acc += sh.rb * sh.splits;
                     g.smem = std::max(g.smem, sh.smem);
                 } else {
-                    const FeatShape fs = batch_feat_shape(P.n, P.m, tpu);
+                    const FeatShape fs = batch_feat_shape(P.n, P.m, tpu, P.fpieces);
                     set_feat_geometry(P, fs);
                     P.grid_ticket = P.rb_ticket + fs.merge_rb;
                     t2.push_back(acc2);
@@ -328,7 +331,7 @@ void scratch_need(Inst &I, int sms) {
             tick = std::max(tick, (size_t)sh.rb + 1);
             blk = std::max(blk, (size_t)sh.rb * 4);
         } else {
-            const FeatShape fs = batch_feat_shape(n, m, 1);
+            const FeatShape fs = batch_feat_shape(n, m, 1, 3);   // narrowest tiles: most slices
             part = std::max(part, fs.part_bytes);
             tick = std::max(tick, (size_t)fs.merge_rb + 1);
             blk = std::max(blk, (size_t)fs.merge_rb * 4);

@@ -171,6 +171,7 @@ struct PassParams {
     // geometry (feature passes: row tiles, column tiles, slices, tiles per slice)
     int nrb;
     int ft_rtiles, ft_ctiles, ft_splits, ft_tps;
+    int ft_rblk, ft_cblk;       // packed 128-point blocks of the row / column clouds
 };
 
 // 2^x on the MUFU pipe (PTX ex2.approx.ftz.f32: relative error ~2^-22, results

@@ -43,19 +43,23 @@ namespace {
 
 using namespace culamp_dev;
 
-constexpr int FT_M = 128;                          // rows per tile = TMEM lanes
-constexpr int FT_N = 128;                          // columns per tile
+constexpr int FT_M = 128;                          // rows per tile = TMEM lanes; packed block height
 constexpr int FT_K = 64;                           // K elements per block (128 bytes of bf16)
 constexpr int FT_PIECE_ELEMS = FT_M * FT_K;        // one 128 x 64 block: 16 KB
 constexpr int FT_PIECE_BYTES = FT_PIECE_ELEMS * 2;
 constexpr int FT_THREADS = 192;
-constexpr int FT_TMEM_COLS = 2 * FT_N;             // two accumulators
 constexpr unsigned long long FT_WAIT_NS = 2000000000ull;
-constexpr int FT_CTRL_BYTES = 8192;                // barriers, TMEM slot, per-warp column terms
+constexpr int FT_CTRL_BYTES = 10240;               // barriers, TMEM slot, per-warp column terms
 
+// N: columns per tile (MMA N, TMEM columns per accumulator). One stage holds
+// the A pieces (NP x 16 KB) and the B pieces (NP x N/128 x 16 KB) of one K
+// block. BF16x3 uses N = 256: each A piece then feeds twice the columns, so
+// two 96 KB stages buffer ~3000 tensor cycles of work against the copies'
+// latency (three 64 KB stages of N = 128 buffered ~2300). BF16x6 keeps
+// N = 128 (two 96 KB stages).
 template <int NP> struct FtCfg;
-template <> struct FtCfg<2> { static constexpr int NS = 3, NPROD = 3; };
-template <> struct FtCfg<3> { static constexpr int NS = 2, NPROD = 6; };
+template <> struct FtCfg<2> { static constexpr int NS = 2, NPROD = 3, N = 256; };
+template <> struct FtCfg<3> { static constexpr int NS = 2, NPROD = 6, N = 128; };
 
 // (A piece, B piece) of product q, small terms first.
 template <int NP>
@@ -173,8 +177,12 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 }
 
 template <int NP>
+__host__ __device__ constexpr size_t ft_stage_bytes() {
+    return (size_t)NP * FT_PIECE_BYTES * (1 + FtCfg<NP>::N / FT_M);
+}
+template <int NP>
 constexpr size_t ft_smem_bytes() {
-    return 1024 + (size_t)FtCfg<NP>::NS * 2 * NP * FT_PIECE_BYTES + FT_CTRL_BYTES;
+    return 1024 + (size_t)FtCfg<NP>::NS * ft_stage_bytes<NP>() + FT_CTRL_BYTES;
 }
 
 // Unit u's parameters: the kernel argument, or (batched) the instance i with
@@ -216,7 +224,11 @@ __global__ void __launch_bounds__(FT_THREADS, 1)
                        const int *unit_start, int count, int total_units, int *batch_err) {
     constexpr int NS = FtCfg<NP>::NS;
     constexpr int NPROD = FtCfg<NP>::NPROD;
-    constexpr uint32_t STAGE = 2u * NP * FT_PIECE_BYTES;
+    constexpr int FT_N = FtCfg<NP>::N;
+    constexpr int NB = FT_N / FT_M;                      // packed blocks per column tile
+    constexpr uint32_t FT_TMEM_COLS = 2u * FT_N;         // two accumulators
+    constexpr uint32_t STAGE = (uint32_t)ft_stage_bytes<NP>();
+    constexpr uint32_t BOFF = (uint32_t)(NP * FT_PIECE_BYTES);   // B pieces after the A pieces
     extern __shared__ unsigned char ft_raw[];
 
     if (!BAT && pass_skipped(P0)) return;
@@ -269,8 +281,8 @@ __global__ void __launch_bounds__(FT_THREADS, 1)
             int local;
             const PassParams &Q = unit_params<BAT>(P0, plist, unit_start, count, u, local);
             if (BAT && pass_skipped(Q)) continue;
-            const int splits = Q.ft_splits, tps = Q.ft_tps, ctiles = Q.ft_ctiles, rtiles = Q.ft_rtiles;
-            const int nkb = Q.fkb;
+            const int splits = Q.ft_splits, tps = Q.ft_tps, ctiles = Q.ft_ctiles;
+            const int rblk = Q.ft_rblk, cblk = Q.ft_cblk, nkb = Q.fkb;
             const int rt = local / splits, sp = local - (local / splits) * splits;
             const int ct0 = sp * tps, ct1 = min(ctiles, ct0 + tps);
             for (int ct = ct0; ok && ct < ct1; ++ct) {
@@ -284,13 +296,15 @@ __global__ void __launch_bounds__(FT_THREADS, 1)
 #pragma unroll
                         for (int p = 0; p < NP; ++p)
                             bulk_g2s(dst + p * FT_PIECE_BYTES,
-                                     Q.fx + ((size_t)(p * rtiles + rt) * nkb + kb) * FT_PIECE_ELEMS,
+                                     Q.fx + ((size_t)(p * rblk + rt) * nkb + kb) * FT_PIECE_ELEMS,
                                      FT_PIECE_BYTES, FULL + 8u * s);
 #pragma unroll
                         for (int p = 0; p < NP; ++p)
-                            bulk_g2s(dst + (NP + p) * FT_PIECE_BYTES,
-                                     Q.fy + ((size_t)(p * ctiles + ct) * nkb + kb) * FT_PIECE_ELEMS,
-                                     FT_PIECE_BYTES, FULL + 8u * s);
+#pragma unroll
+                            for (int hb = 0; hb < NB; ++hb)
+                                bulk_g2s(dst + BOFF + (p * NB + hb) * FT_PIECE_BYTES,
+                                         Q.fy + ((size_t)(p * cblk + ct * NB + hb) * nkb + kb) * FT_PIECE_ELEMS,
+                                         FT_PIECE_BYTES, FULL + 8u * s);
 #pragma unroll
                         for (int s2 = 0; s2 < NS; ++s2)
                             if (s2 == s) last_use[s2] = (int)use;
@@ -340,7 +354,7 @@ __global__ void __launch_bounds__(FT_THREADS, 1)
 #pragma unroll
                             for (int k4 = 0; k4 < FT_K / 16; ++k4) {
                                 const uint64_t ad = sw128_desc(sa + pa * FT_PIECE_BYTES + k4 * 32);
-                                const uint64_t bd = sw128_desc(sa + (NP + pb) * FT_PIECE_BYTES + k4 * 32);
+                                const uint64_t bd = sw128_desc(sa + BOFF + pb * NB * FT_PIECE_BYTES + k4 * 32);
                                 umma_bf16(dacc, ad, bd, idesc, (kb | q | k4) != 0 ? 1u : 0u);
                             }
                         }
@@ -651,19 +665,28 @@ namespace culamp_host {
 
 int feat_kblocks(int d) { return (d + FT_K - 1) / FT_K; }
 
+// 128-point blocks of a packed cloud: an even count, so that any cloud can be
+// read as 256-column tiles (zero points pad the last block pair).
+int feat_blocks(int n) { return 2 * ((n + 2 * FT_M - 1) / (2 * FT_M)); }
+
+int feat_tile_cols(int pieces) { return pieces == 2 ? FtCfg<2>::N : FtCfg<3>::N; }
+
 size_t feat_piece_elems(int n, int d, int pieces) {
-    const size_t tiles = (size_t)((n + FT_M - 1) / FT_M);
-    return (size_t)pieces * tiles * FT_M * (size_t)feat_kblocks(d) * FT_K;
+    return (size_t)pieces * (size_t)feat_blocks(n) * FT_M * (size_t)feat_kblocks(d) * FT_K;
 }
 
-// Work units: 128-row tiles x slices of 128-column tiles. The slice count is
+// Work units: 128-row tiles x slices of N-column tiles. The slice count is
 // the smallest that minimises the tiles of the busiest CTA (one CTA per SM),
 // plus a small charge per slice for the partials and their merge.
-FeatShape feat_shape(int n, int m, int sm_count) {
+FeatShape feat_shape(int n, int m, int sm_count, int pieces) {
     FeatShape fs{};
     const int sms = sm_count > 0 ? sm_count : 148;
+    const int N = feat_tile_cols(pieces);
     fs.rtiles = (n + FT_M - 1) / FT_M;
-    fs.ctiles = (m + FT_N - 1) / FT_N;
+    fs.ctiles = (m + N - 1) / N;
+    fs.rblk = feat_blocks(n);
+    fs.cblk = feat_blocks(m);
+    fs.ncols = N;
     double best = 1e300;
     const int smax = fs.ctiles < 64 ? fs.ctiles : 64;
     for (int s = 1; s <= smax; ++s) {
@@ -688,7 +711,7 @@ FeatShape feat_shape(int n, int m, int sm_count) {
 
 cudaError_t feat_prepare(uint16_t *pieces, double *norms, const double *X, int n, int d, int np,
                          cudaStream_t st) {
-    const int tiles = (n + FT_M - 1) / FT_M;
+    const int tiles = feat_blocks(n);
     const int nkb = feat_kblocks(d);
     const long long total = (long long)tiles * FT_M * nkb * 8;
     feat_pack_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(pieces, X, n, d, tiles, nkb, np);
@@ -701,7 +724,7 @@ cudaError_t feat_prepare(uint16_t *pieces, double *norms, const double *X, int n
 cudaError_t launch_feat_pass(PassParams P, int acc, Scratch &scr, int sm_count, cudaStream_t st) {
     if (!P.fx || !P.fy || !P.xn || !P.yn || P.fkb < 1 || (P.fpieces != 2 && P.fpieces != 3))
         return cudaErrorInvalidValue;
-    const FeatShape fs = feat_shape(P.n, P.m, sm_count);
+    const FeatShape fs = feat_shape(P.n, P.m, sm_count, P.fpieces);
     if (scr.part.bytes < fs.part_bytes || scr.tickets.bytes < (size_t)(fs.merge_rb + 1) * sizeof(unsigned) ||
         scr.blk.bytes < (size_t)fs.merge_rb * 4 * sizeof(double))
         return cudaErrorInvalidValue;
@@ -716,10 +739,12 @@ cudaError_t launch_feat_pass(PassParams P, int acc, Scratch &scr, int sm_count, 
 
 void set_feat_geometry(PassParams &P, const FeatShape &fs) {
     P.splits = fs.splits;
-    P.cols_per_split = fs.tps * FT_N;
+    P.cols_per_split = fs.tps * fs.ncols;
     P.nrb = fs.merge_rb;
     P.ft_rtiles = fs.rtiles;
     P.ft_ctiles = fs.ctiles;
+    P.ft_rblk = fs.rblk;
+    P.ft_cblk = fs.cblk;
     P.ft_splits = fs.splits;
     P.ft_tps = fs.tps;
 }

@@ -85,14 +85,18 @@ int pmode_of(double p);   // P_L1 / P_SQ / P_INF / P_GEN
 constexpr int FEAT_MIN_D = 32;
 
 struct FeatShape {
-    int rtiles, ctiles;   // 128-row tiles of the output rows, 128-column tiles
+    int rtiles, ctiles;   // 128-row tiles of the output rows, ncols-column tiles
+    int rblk, cblk;       // 128-point blocks of the packed row / column clouds (piece strides)
+    int ncols;            // columns per tile (MMA N)
     int splits, tps;      // column slices, column tiles per slice
     int units, grid;      // work units (row tile x slice), CTAs (<= SMs)
     int merge_rb;         // CTAs of the merge / epilogue kernel
     size_t part_bytes;    // partials: splits * n * 3 doubles
 };
 
-FeatShape feat_shape(int n, int m, int sm_count);
+FeatShape feat_shape(int n, int m, int sm_count, int pieces);
+int feat_blocks(int n);                 // 128-point blocks of a packed cloud (even)
+int feat_tile_cols(int pieces);         // columns per tile for BF16x3 (2) / BF16x6 (3)
 int feat_kblocks(int d);
 size_t feat_piece_elems(int n, int d, int pieces);   // bf16 elements of one packed cloud
 // Pack one cloud (n x d, FP64) into `pieces` bf16 pieces and its squared norms.

@@ -195,7 +195,7 @@ int ensure_solver(culamp_handle h, int n, int m, int d, int64_t log_cap, int fea
             nrb = (size_t)sh.rb > nrb ? (size_t)sh.rb : nrb;
         }
     if (feat_np > 0)
-        for (const FeatShape &fs : {feat_shape(n, m, h->sm_count), feat_shape(m, n, h->sm_count)}) {
+        for (const FeatShape &fs : {feat_shape(n, m, h->sm_count, feat_np), feat_shape(m, n, h->sm_count, feat_np)}) {
             pb = fs.part_bytes > pb ? fs.part_bytes : pb;
             nrb = (size_t)fs.merge_rb > nrb ? (size_t)fs.merge_rb : nrb;
         }
