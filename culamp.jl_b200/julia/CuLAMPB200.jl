@@ -19,6 +19,9 @@ const CULAMP_FLAG_TRUE_PINF = UInt32(1)
 const CULAMP_FLAG_CHECK_ALWAYS = UInt32(2)
 const CULAMP_FLAG_MARGINAL_ONLY = UInt32(4)
 const CULAMP_FLAG_FORM_PLAIN = UInt32(8)
+const CULAMP_FLAG_NO_GRAPH = UInt32(16)
+const CULAMP_FLAG_FEAT_X6 = UInt32(32)
+const CULAMP_FLAG_FEAT_FP64 = UInt32(64)
 
 # struct culamp_args (EOTArgs, src/Utilities.jl:18-31)
 struct CArgs
@@ -160,6 +163,84 @@ function annealed_sinkhorn_euclidean(marginal1::CuArray{Float64}, marginal2::CuA
         open(potentials * ".col", "w") do f; foreach(v -> println(f, v), ψ_out); end
     end
     return φ_out, ψ_out, stats.objective
+end
+
+# ---------------------------------------------------------------- batched solves
+
+struct CInstance
+    x::CuPtr{Float64}; y::CuPtr{Float64}; r::CuPtr{Float64}; c::CuPtr{Float64}
+    phi::CuPtr{Float64}; psi::CuPtr{Float64}; n::Int64; m::Int64; d::Int32; reserved::Int32
+end
+
+struct CBatchStats
+    iterations::Int64; num_iter::Int64; residual::Float64; objective::Float64; winf::Float64
+    stopped::Int32; status::Int32
+end
+
+mutable struct CBatchInfo
+    elapsed_ms::Float64; tune_ms::Float64; target_ctas_per_sm::Int32; feat_tiles_per_unit::Int32
+    unroll::Int32; launches_per_iteration::Int32; phases::Int32; reserved::Int32
+    CBatchInfo() = new(0.0, 0.0, 0, 0, 0, 0, 0, 0)
+end
+
+"""
+    batched_sinkhorn(xs, ys, rs, cs, args, frequency=100, p=2; flags=0)
+
+Many independent kernel Sinkhorn problems (each as in sinkhorn_color_transfer,
+SinkhornKernel.jl:477-559) of uneven sizes in one culamp_batched_sinkhorn call.
+xs[k] is d x N_k, ys[k] d x M_k (CuArray{Float64}); returns (φs, ψs, stats).
+"""
+function batched_sinkhorn(xs, ys, rs, cs, args, frequency::Int=100, p=2; flags::UInt32=UInt32(0))
+    K = length(xs)
+    φs = [CUDA.zeros(Float64, size(xs[k], 2)) for k in 1:K]
+    ψs = [CUDA.zeros(Float64, size(ys[k], 2)) for k in 1:K]
+    insts = [CInstance(pointer(xs[k]), pointer(ys[k]), pointer(rs[k]), pointer(cs[k]), pointer(φs[k]),
+                       pointer(ψs[k]), size(xs[k], 2), size(ys[k], 2), size(xs[k], 1), 0) for k in 1:K]
+    stats = Vector{CBatchStats}(undef, K)
+    info = Ref(CBatchInfo())
+    cargs = Ref(CArgs(args))
+    check(ccall((:culamp_batched_sinkhorn, libculamp), Cint,
+                (Ptr{Cvoid}, Ptr{CInstance}, Int32, Ptr{CArgs}, Int64, Float64, UInt32,
+                 Ptr{CBatchStats}, Ref{CBatchInfo}, Ptr{Cvoid}),
+                handle(), insts, K, cargs, frequency, Float64(p), flags, stats, info, stream_ptr()))
+    return φs, ψs, stats
+end
+
+# ---------------------------------------------------------------- gradients
+
+"""
+    adjoint_sk(x, y, φ, ψ, eps, p=2) -> grad (d x N)
+
+sum_j P_ij grad_x C(x_i, y_j) for P_ij = exp(φ_i + ψ_j - C_ij / eps) (eps
+absolute), one pass over all pairs without storing P (culamp_adjoint_sk). With
+solved potentials this is dOT_eps/dx (envelope theorem); dOT/dy is
+adjoint_sk(y, x, ψ, φ, eps, p), dOT/da = eps φ, dOT/db = eps ψ.
+"""
+function adjoint_sk(x::CuArray{Float64}, y::CuArray{Float64}, φ::CuArray{Float64}, ψ::CuArray{Float64},
+                    eps::Float64, p=2)
+    d, N = size(x)
+    M = size(y, 2)
+    g = CUDA.zeros(Float64, d, N)
+    check(ccall((:culamp_adjoint_sk, libculamp), Cint,
+                (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, CuPtr{Float64}, CuPtr{Float64}, Int64, Int64,
+                 Int32, CuPtr{Float64}, CuPtr{Float64}, Float64, Float64, Float64, Ptr{Cvoid}),
+                handle(), g, CU_NULL, x, y, N, M, d, φ, ψ, eps, 1.0, Float64(p), stream_ptr()))
+    return g
+end
+
+"""
+    lse_combine!(ψ, parts)
+
+Column potentials of a row-sharded Sinkhorn from the shards' column passes:
+ψ_j = -log sum_g exp(-parts[j, g]) (parts: M x G, one column per shard, e.g. an
+all-gather of the shards' outputs; culamp_lse_combine).
+"""
+function lse_combine!(ψ::CuArray{Float64}, parts::CuArray{Float64})
+    M, G = size(parts)
+    check(ccall((:culamp_lse_combine, libculamp), Cint,
+                (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Int32, Int64, Ptr{Cvoid}),
+                handle(), ψ, parts, G, M, stream_ptr()))
+    return ψ
 end
 
 end # module
