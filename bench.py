@@ -534,7 +534,8 @@ def extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_chosen, chosen_ms):
 def divergence_extra(cb, D, torch, dev, X, Y, R, Cc, winf_xy):
     """Sinkhorn divergence S = OT(a,b) - OT(a,a)/2 - OT(b,b)/2 of the 65536-point
     RGB clouds at eps = eta_p * W_inf(x, y) (absolute, shared by the three
-    solves, each to 1e-6 L1), then dS/dx, dS/dy by the adjoint pass (six passes
+    solves, each to 1e-6 L1; the self terms by the symmetric iteration, one
+    averaged row pass per iteration), then dS/dx, dS/dy by the adjoint pass (six passes
     over n*m pairs, P_ij recomputed, nothing n x m stored) and dS/da, dS/db
     from the potentials. Device time with CUDA events."""
     from culamp_b200.divergence import divergence_grads, sinkhorn_divergence

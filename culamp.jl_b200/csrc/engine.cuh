@@ -72,6 +72,7 @@ enum Epi {
     EPI_LOGZ = 2,        // out = L; aux = log(marg) - L (if marg)       (a7)
     EPI_SPP_COL = 3,     // res = exp(-rowpot/eta_t + L); cost = res*E[C] (a8) [+ LAMP step]
     EPI_RAW = 4,         // out = value (max / min reductions)            (a6, a9)
+    EPI_SK_SYM = 5,      // symmetric step: out = (f + log(marg) - L)/2; res at f; aux = L
 };
 
 enum LampStep { LAMP_NONE = 0, LAMP_A = 1, LAMP_B = 2 };
@@ -86,6 +87,7 @@ enum Finish {
     FIN_LAMP_DUAL = 6,   // LAMP dual pass: primal/dual, log, tolerance test
     FIN_LAMP_B = 7,      // LAMP column pass after infeas(nu_bar): commit eta_t, iteration
     FIN_MAXCOST = 8,     // W_inf = max of row maxima into ctl->winf
+    FIN_SK_SYM = 9,      // symmetric Sinkhorn pass: tolerance test, iteration bookkeeping
 };
 
 // Gate: when the kernel runs.
@@ -528,6 +530,22 @@ static __device__ __noinline__ void run_finish(const PassParams &P, const double
             }
             break;
         }
+        case FIN_SK_SYM: {
+            // tot[0] = L1 row residual at the pass's input f, tot[2] = a.f. On
+            // success f is final and iter counts the updates applied before it.
+            const double l1 = tot[0];
+            c->residual = l1;
+            c->dualval = tot[2];
+            if (c->log && (c->iter % c->frequency) == 0)
+                put_log(c, (double)c->iter, l1, nan(""), nan(""), 2.0 * tot[2]);
+            if (l1 <= c->epsilon / 6.0) { c->stop = 1; c->stop_reason = 1; }
+            else {
+                end_of_iteration(c);
+                c->num_iter = c->iter;
+                if (c->pending_stop) { c->stop = 1; c->stop_reason = c->pending_stop; }
+            }
+            break;
+        }
         case FIN_LAMP_Z:
             c->sum_r_logz = tot[0];
             break;
@@ -698,6 +716,7 @@ constexpr int FR_HHI = FR_H0 + 126;
 __device__ __forceinline__ double row_reference(const PassParams &P, int o, double beta) {
     if (P.epi == EPI_SK_ROW) return log(P.marg[o]) - P.out[o];
     if (P.epi == EPI_LOGZ) return P.out[o];
+    if (P.epi == EPI_SK_SYM) return P.aux ? P.aux[o] : NAN;
     if (P.epi == EPI_SPP_COL)
         return log(P.out[o]) - ((beta == 0.0 || !P.rowpot) ? 0.0 : beta * P.rowpot[o]);
     return NAN;
@@ -936,6 +955,20 @@ __device__ __forceinline__ void row_epilogue(const PassParams &P, int rb, int ro
                 acc4[0] += fabs(res);
                 acc4[1] += mass * Ec;
                 acc4[2] += P.marg[o] * P.rowpot[o];
+                break;
+            }
+            case EPI_SK_SYM: {
+                // f = rowpot = colpot (x against itself): T(f)_i = log a_i - L_i
+                // and the row mass of P_ij = exp(f_i + f_j - C_ij/eps) is
+                // a_i exp(f_i - T(f)_i); the next f is the average (f + T(f))/2
+                const double f = P.rowpot[o];
+                const double T = log(P.marg[o]) - L;
+                const double mass = exp(f + L);
+                P.out[o] = 0.5 * (f + T);
+                if (P.aux) P.aux[o] = L;
+                acc4[0] += fabs(P.marg[o] - mass);
+                acc4[1] += mass * Ec;
+                acc4[2] += P.marg[o] * f;
                 break;
             }
             case EPI_LOGZ: {

@@ -60,7 +60,7 @@ __global__ void loop_ctl_kernel(Ctl *c, cudaGraphConditionalHandle hnd) {
 
 }  // namespace culamp_dev
 
-enum SolverKind { KIND_SK = 1, KIND_LAMP = 2 };
+enum SolverKind { KIND_SK = 1, KIND_LAMP = 2, KIND_SYM = 3 };
 
 // Everything a captured graph bakes into kernel parameters.
 struct GraphKey {
@@ -603,6 +603,159 @@ extern "C" int culamp_sinkhorn(culamp_handle h, const double *x, const double *y
         fill_stats_common(stats, hc, ms);
         stats->residual = resid;
         stats->objective = obj;
+        stats->winf = winf;
+        stats->eta_t = NAN;
+        stats->s_t = NAN;
+    }
+    return CULAMP_OK;
+}
+
+// -------------------------------------------------------- symmetric Sinkhorn
+
+// Self-transport OT(a, a; x, x): the optimal plan is symmetric, so one
+// potential f (P_ij = exp(f_i + f_j - C_ij/(eta_p W_inf))) solves it. Each
+// iteration is ONE row pass, f <- (f + T(f))/2 with T(f) = log a - LSE_j(
+// -C_ij/(eta_p W_inf) + f_j); its fixed point is the symmetric Sinkhorn
+// solution and the averaged map converges in a few dozen passes where the
+// alternating iteration needs hundreds. The same pass yields the L1 row
+// residual at its input f, a_i |1 - exp(f_i - T(f)_i)| summed, so every
+// iteration is checked. The two potential buffers alternate as input and output.
+extern "C" int culamp_symmetric_sinkhorn(culamp_handle h, const double *x, int64_t n, int32_t d,
+                                         const double *r, const culamp_args *args, int64_t frequency,
+                                         double p, const double *f0, uint32_t flags, double *f,
+                                         culamp_stats *stats, culamp_log_row *log, int64_t log_cap,
+                                         void *stream) {
+    int s = check_solver_args(h, x, x, n, n, d, r, r, args, frequency, p);
+    if (s) return s;
+    if (!f) return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "null output pointer");
+    if (!(args->eta_p > 0.0))
+        return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "Sinkhorn needs eta_p > 0 (got %g)", args->eta_p);
+    if (flags & CULAMP_FLAG_FORM_PLAIN)
+        return culamp_set_error(h, CULAMP_ERR_UNSUPPORTED, "symmetric solve has no plain form");
+    cudaStream_t st = (cudaStream_t)stream;
+    s = ensure_solver(h, (int)n, (int)n, d, log ? log_cap : 0, feat_pieces(d, flags));
+    if (s) return s;
+    Solver &S = *h->solver;
+    int dk = d;
+    s = stage_inputs(h, x, x, (int)n, (int)n, d, r, r, st, nullptr, &dk);
+    if (s) return s;
+    d = dk;
+    s = prepare_features(h, (int)n, (int)n, d, st);
+    if (s) return s;
+    if (f0) CUDA_TRY(h, cudaMemcpyAsync(S.phi.ptr, f0, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    else CUDA_TRY(h, cudaMemsetAsync(S.phi.ptr, 0, n * sizeof(double), st));
+    // all-ones bytes are a NaN: no fixed-reference hint before the first pass
+    CUDA_TRY(h, cudaMemsetAsync(S.aux.ptr, 0xFF, n * sizeof(double), st));
+    double winf = 0.0;
+    s = compute_winf(h, (int)n, (int)n, d, p, st, &winf);
+    if (s) return s;
+
+    Ctl c;
+    std::memset(&c, 0, sizeof(c));
+    c.itermax = args->itermax;
+    c.frequency = frequency;
+    c.stop = args->itermax < 1;
+    c.stop_reason = args->itermax < 1 ? 2 : 0;
+    c.tmax_s = args->tmax;
+    c.epsilon = args->epsilon;
+    c.eta = args->eta_p;
+    c.winf = winf;
+    c.log = log ? S.logbuf.as<culamp_log_row>() : nullptr;
+    c.log_cap = log ? log_cap : 0;
+    CUDA_TRY(h, cudaMemcpyAsync(S.ctl.ptr, &c, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+    set_start_kernel<<<1, 1, 0, st>>>(S.ctl.as<Ctl>());
+
+    const bool true_pinf = flags & CULAMP_FLAG_TRUE_PINF;
+    const double p_iter = (std::isinf(p) && !true_pinf) ? 2.0 : p;   // as the Sinkhorn iteration
+    const double p_res = true_pinf ? p : (p == 1.0 ? 1.0 : 2.0);      // as its residual pass
+    const int pm = pmode_of(p_iter), pm_res = pmode_of(p_res);
+    double *X = S.X.as<double>();
+    PassParams pa = mk(X, X, (int)n, (int)n, d, p_iter, S.ctl.as<Ctl>());
+    pa.ctr = X;
+    pa.epi = EPI_SK_SYM;
+    pa.coef_mode = COEF_SK;
+    pa.marg = S.r.as<double>();
+    pa.aux = S.aux.as<double>();
+    pa.use_ref = 1;
+    pa.finish = FIN_SK_SYM;
+    apply_feat(S, pa, true);
+    PassParams pb = pa;
+    pa.colpot = pa.rowpot = S.phi.as<double>();
+    pa.out = S.psi.as<double>();
+    pb.colpot = pb.rowpot = S.psi.as<double>();
+    pb.out = S.phi.as<double>();
+    const LaunchShape sh = pass_shape((int)n, (int)n, d, ACC_LSE, h->sm_count);
+    int unroll = pick_unroll((double)n * n);
+    unroll += unroll & 1;   // every graph body starts on the phi -> psi pass
+    int pos = 0;
+    auto body = [&](cudaStream_t sx) -> cudaError_t {
+        const PassParams &P = (pos & 1) ? pb : pa;
+        pos += 1;
+        return launch_pass(P, pm, ACC_LSE, sh, S.scr, sx);
+    };
+    CUDA_TRY(h, cudaEventRecord(S.ev0, st));
+    if (flags & CULAMP_FLAG_NO_GRAPH) {
+        for (long long it = 0; it < args->itermax + 2; ++it) {
+            CUDA_TRY(h, body(st));
+            int stop = 0;
+            CUDA_TRY(h, cudaMemcpyAsync(&stop, &S.ctl.as<Ctl>()->stop, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CUDA_TRY(h, cudaStreamSynchronize(st));
+            if (stop) break;
+        }
+    } else {
+        GraphKey key;
+        key.kind = KIND_SYM;
+        key.n = key.m = (int)n;
+        key.d = d;
+        key.pm_iter = pm;
+        key.p = p;
+        key.feat = S.feat_active ? S.feat_np : 0;
+        key.unroll = unroll;
+        key.generation = S.generation;
+        cudaGraphExec_t ex = nullptr;
+        pos = 0;
+        s = get_graph(h, key, body, &ex);
+        if (s) return s;
+        CUDA_TRY(h, cudaGraphLaunch(ex, st));
+    }
+    CUDA_TRY(h, cudaEventRecord(S.ev1, st));
+    Ctl hc;
+    CUDA_TRY(h, cudaMemcpyAsync(&hc, S.ctl.ptr, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    float ms = 0.f;
+    CUDA_TRY(h, cudaEventElapsedTime(&ms, S.ev0, S.ev1));
+    if (hc.error) return culamp_set_error(h, CULAMP_ERR_DEVICE_TIMEOUT, "loop control bound hit");
+    // pass t reads buffer t % 2; iter = updates applied = the buffer holding the result
+    const double *fres = (hc.iter & 1) ? S.psi.as<double>() : S.phi.as<double>();
+
+    // residual and transport cost at the returned f (the Sinkhorn residual pass)
+    PassParams pr = mk(X, X, (int)n, (int)n, d, p_res, h->pass_ctl.as<Ctl>());
+    pr.ctr = X;
+    pr.epi = EPI_SK_RESID;
+    pr.coef_mode = COEF_FIXED;
+    pr.alpha = -1.0 / (args->eta_p * winf);
+    pr.beta = 1.0;
+    pr.colpot = fres;
+    pr.rowpot = fres;
+    pr.marg = S.r.as<double>();
+    pr.out = S.res.as<double>();
+    pr.out2 = S.cost.as<double>();
+    pr.want_moment = 1;
+    pr.finish = FIN_SUMS;
+    apply_feat(S, pr, true);
+    CUDA_TRY(h, launch_pass(pr, pm_res, ACC_LSE, pass_shape((int)n, (int)n, d, ACC_LSE, h->sm_count, true),
+                            S.scr, st));
+    double sums[4];
+    CUDA_TRY(h, cudaMemcpyAsync(sums, h->pass_ctl.as<Ctl>()->sums, sizeof(sums), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaMemcpyAsync(f, fres, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    s = copy_log(h, hc, log, log_cap, st);
+    if (s) return s;
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        fill_stats_common(stats, hc, ms);
+        stats->residual = sums[0];
+        stats->objective = sums[1];
         stats->winf = winf;
         stats->eta_t = NAN;
         stats->s_t = NAN;

@@ -12,7 +12,7 @@ from .solvers import (BatchResult, Handle, SolveResult, annealed_sinkhorn_euclid
                       extragradient_color_transfer, extragradient_euclidean, get_handle,
                       lamp_barycentric_maps, marginal_error_fp64, sinkhorn_color_transfer,
                       sinkhorn_euclidean, solve_annealed_sinkhorn, solve_batched_sinkhorn, solve_lamp,
-                      solve_sinkhorn)
+                      solve_sinkhorn, solve_symmetric_sinkhorn)
 from . import kernels
 
 __all__ = [
@@ -23,5 +23,5 @@ __all__ = [
     "annealed_sinkhorn_euclidean", "barycentric_map", "extragradient_color_transfer",
     "extragradient_euclidean", "get_handle", "lamp_barycentric_maps", "marginal_error_fp64",
     "sinkhorn_color_transfer", "sinkhorn_euclidean", "solve_annealed_sinkhorn", "solve_lamp",
-    "solve_batched_sinkhorn", "solve_sinkhorn", "kernels",
+    "solve_batched_sinkhorn", "solve_sinkhorn", "solve_symmetric_sinkhorn", "kernels",
 ]

@@ -111,6 +111,8 @@ SIGNATURES = {
     "culamp_annealed_sinkhorn": (C.c_int, [_VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP,
                                            C.POINTER(CArgs), _I64, _D, _U32, _VP, _VP,
                                            C.POINTER(CStats), C.POINTER(CLogRow), _I64, _VP]),
+    "culamp_symmetric_sinkhorn": (C.c_int, [_VP, _VP, _I64, _I32, _VP, C.POINTER(CArgs), _I64, _D, _VP,
+                                            _U32, _VP, C.POINTER(CStats), C.POINTER(CLogRow), _I64, _VP]),
     "culamp_sinkhorn_host": (C.c_int, [_VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, C.POINTER(CArgs),
                                        _I64, _D, _VP, _VP, _U32, _VP, _VP, C.POINTER(CStats),
                                        C.POINTER(CLogRow), _I64]),

@@ -14,8 +14,12 @@ Gradients (envelope theorem, eps fixed -- W_inf does not enter):
   * d OT / d a_i = eps phi_i, d OT / d b_j = eps psi_j (the potentials; defined
     up to a constant because sum a = sum b = 1).
 
-S_eps(a, b) = OT(a, b) - OT(a, a)/2 - OT(b, b)/2. In OT(a, a; x, x) the cloud x
-enters both sides, so its gradient is the row pass plus the column pass.
+S_eps(a, b) = OT(a, b) - OT(a, a)/2 - OT(b, b)/2. The self terms have a
+symmetric optimal plan and one potential f = phi = psi; they are solved by the
+averaged symmetric iteration f <- (f + T(f))/2 (culamp_symmetric_sinkhorn), one
+row pass per iteration, which reaches the tolerance in tens of passes where
+the alternating iteration takes hundreds. In OT(a, a; x, x) the cloud x enters
+both sides, so its gradient is the row pass plus the column pass.
 
 SinkhornDivergence is a torch.autograd.Function -- the Python counterpart of a
 ChainRulesCore rrule.
@@ -29,7 +33,7 @@ import torch
 
 from . import kernels as K
 from .args import EOTArgs
-from .solvers import _dev, _stream, get_handle, solve_sinkhorn
+from .solvers import _dev, _stream, get_handle, solve_sinkhorn, solve_symmetric_sinkhorn
 
 
 @dataclass
@@ -52,6 +56,17 @@ def entropic_ot(x, y, a, b, eps: float, p: float = 2.0, tol: float = 1e-7, frequ
     args = EOTArgs(eta_p=eta_p, epsilon=6.0 * tol, itermax=itermax, verbose=False)
     res = solve_sinkhorn(x, y, a, b, args, frequency, p, phi0=phi0, psi0=psi0)
     value = eps * (float(torch.dot(a, res.phi)) + float(torch.dot(b, res.psi)))
+    return OTResult(value, res.phi, res.psi, eps, eta_p, winf, res.iterations, res.residual)
+
+
+def entropic_ot_self(x, a, eps: float, p: float = 2.0, tol: float = 1e-7, frequency: int = 10,
+                     itermax: int = 200_000, f0=None) -> OTResult:
+    """OT_eps(a, a; x, x) by the symmetric iteration, to L1 marginal error tol."""
+    _, winf = K.max_logsumexp_spp_ct(x, x, p)
+    eta_p = eps / winf
+    args = EOTArgs(eta_p=eta_p, epsilon=6.0 * tol, itermax=itermax, verbose=False)
+    res = solve_symmetric_sinkhorn(x, a, args, frequency, p, f0=f0)
+    value = 2.0 * eps * float(torch.dot(a, res.phi))
     return OTResult(value, res.phi, res.psi, eps, eta_p, winf, res.iterations, res.residual)
 
 
@@ -84,10 +99,8 @@ def sinkhorn_divergence(x, y, a, b, eps: float, p: float = 2.0, tol: float = 1e-
     w = warm or (None, None, None)
     xy = entropic_ot(x, y, a, b, eps, p, tol, frequency,
                      phi0=w[0].phi if w[0] else None, psi0=w[0].psi if w[0] else None)
-    xx = entropic_ot(x, x, a, a, eps, p, tol, frequency,
-                     phi0=w[1].phi if w[1] else None, psi0=w[1].psi if w[1] else None)
-    yy = entropic_ot(y, y, b, b, eps, p, tol, frequency,
-                     phi0=w[2].phi if w[2] else None, psi0=w[2].psi if w[2] else None)
+    xx = entropic_ot_self(x, a, eps, p, tol, frequency, f0=w[1].phi if w[1] else None)
+    yy = entropic_ot_self(y, b, eps, p, tol, frequency, f0=w[2].phi if w[2] else None)
     return DivergenceParts(xy.value - 0.5 * xx.value - 0.5 * yy.value, xy, xx, yy)
 
 

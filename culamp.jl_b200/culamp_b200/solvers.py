@@ -191,6 +191,31 @@ def solve_sinkhorn(x, y, r, c, args: EOTArgs, frequency: int = 100, p: float = 2
                        log=_log_rows(buf, stats))
 
 
+def solve_symmetric_sinkhorn(x, r, args: EOTArgs, frequency: int = 100, p: float = 2.0, f0=None,
+                             flags: int = 0, handle: Handle | None = None,
+                             log_cap: int = _LOG_CAP) -> SolveResult:
+    """Self-transport OT(r, r; x, x) by the averaged symmetric iteration
+    f <- (f + T(f))/2 (culamp_symmetric_sinkhorn); phi and psi of the result
+    are the same tensor f. Device tensors only."""
+    import torch
+    n, d = _points(x)
+    if not _is_torch(x):
+        raise TypeError("solve_symmetric_sinkhorn takes device tensors")
+    a = args.to_c()
+    stats = _lib.CStats()
+    buf = (_lib.CLogRow * max(1, log_cap))()
+    h = handle or get_handle(x.device.index)
+    f = torch.empty(n, dtype=torch.float64, device=x.device)
+    st = h._lib.culamp_symmetric_sinkhorn(
+        h.ptr, _dev(x, "x", n, 2), n, d, _dev(r, "r", n, 1), C.byref(a), int(frequency), float(p),
+        _dev(f0, "f0", n, 1) if f0 is not None else None, int(flags), C.c_void_p(f.data_ptr()),
+        C.byref(stats), buf, log_cap, _stream())
+    h.check(st, "culamp_symmetric_sinkhorn")
+    return SolveResult(f, f, stats.residual, stats.objective, int(stats.iterations),
+                       int(stats.num_iter), stats.winf, stats.elapsed_ms, int(stats.stopped),
+                       log=_log_rows(buf, stats))
+
+
 def sinkhorn_color_transfer(img1, img2, marginal1, marginal2, args: EOTArgs, frequency: int = 100,
                             p: float = 2, *, return_cuda: bool = False,
                             return_assignments: bool = True, phi0=None, psi0=None,

@@ -206,6 +206,27 @@ function batched_sinkhorn(xs, ys, rs, cs, args, frequency::Int=100, p=2; flags::
     return φs, ψs, stats
 end
 
+"""
+    symmetric_sinkhorn(x, marginal, args, frequency=100, p=2; flags=0) -> (f, stats)
+
+Self-transport OT(a, a; x, x) (the symmetric terms of the Sinkhorn divergence)
+by the averaged iteration f <- (f + T(f))/2, one row pass per iteration
+(culamp_symmetric_sinkhorn); P_ij = exp(f_i + f_j - C_ij / (eta_p W_inf)).
+"""
+function symmetric_sinkhorn(x::CuArray{Float64}, marginal::CuArray{Float64}, args,
+                            frequency::Int=100, p=2; flags::UInt32=UInt32(0))
+    d, N = size(x)
+    f = CUDA.zeros(Float64, N)
+    stats = CStats()
+    cargs = Ref(CArgs(args))
+    check(ccall((:culamp_symmetric_sinkhorn, libculamp), Cint,
+                (Ptr{Cvoid}, CuPtr{Float64}, Int64, Int32, CuPtr{Float64}, Ptr{CArgs}, Int64, Float64,
+                 CuPtr{Float64}, UInt32, CuPtr{Float64}, Ref{CStats}, Ptr{CLogRow}, Int64, Ptr{Cvoid}),
+                handle(), x, N, d, marginal, cargs, frequency, Float64(p), CU_NULL, flags, f, stats,
+                C_NULL, 0, stream_ptr()))
+    return f, stats
+end
+
 # ---------------------------------------------------------------- gradients
 
 """

@@ -206,6 +206,22 @@ int culamp_annealed_sinkhorn(culamp_handle h, const double *x, const double *y, 
                              uint32_t flags, double *phi, double *psi, culamp_stats *stats,
                              culamp_log_row *log, int64_t log_cap, void *stream);
 
+/* Self-transport OT(r, r; x, x), the two symmetric terms of the Sinkhorn
+ * divergence. No counterpart in the reference. The plan is symmetric, so one
+ * potential f solves it (P_ij = exp(f_i + f_j - C_ij/(eta_p W_inf)), W_inf of x
+ * against itself); each iteration is one row pass f <- (f + T(f))/2 with T the
+ * row update of SinkhornKernel.jl:518-520, checked every pass against the L1
+ * row residual at its input (stop at residual <= epsilon/6, as culamp_sinkhorn).
+ * stats: iterations = averaged updates applied; residual / objective from the
+ * Sinkhorn residual pass at the returned f. f0 (device, may be NULL) warm-starts;
+ * `frequency` only paces the log. flags: FEAT_X6 / FEAT_FP64 / NO_GRAPH /
+ * TRUE_PINF. */
+int culamp_symmetric_sinkhorn(culamp_handle h, const double *x, int64_t n, int32_t d,
+                              const double *r, const culamp_args *args, int64_t frequency,
+                              double p, const double *f0, uint32_t flags, double *f,
+                              culamp_stats *stats, culamp_log_row *log, int64_t log_cap,
+                              void *stream);
+
 /* Row-sharded Sinkhorn (several GPUs, or several row blocks on one): shard g's
  * column pass (culamp_lse_rows_sk over its rows) gives out_g = log c - LSE over
  * its rows; the column potential is the log-sum-exp over shards,

@@ -379,6 +379,33 @@ def np_sinkhorn_kernel(x, y, r, c, eta_p, itermax, frequency=1, epsilon=0.0, p=2
     return phi, psi, np.abs(r - P.sum(1)).sum(), (P * Cr).sum(), it_done, winf
 
 
+def np_symmetric_sinkhorn(x, r, eta_p, itermax, epsilon=0.0, p=2.0, f0=None, cost=None, winf=None):
+    """Self-transport OT(r, r; x, x) by the averaged symmetric iteration
+    f <- (f + T(f))/2, T(f) = log r - LSE_j(-C_ij/(eta_p W) + f_j): the row
+    update of SinkhornKernel.jl:518-520 with both potentials equal. No
+    counterpart in the reference; its fixed point is the Sinkhorn solution with
+    phi = psi. Every iteration first tests the L1 row residual at its input f
+    (residual <= epsilon/6 stops before updating). Returns (f, residual at f,
+    transport cost at f, updates applied, W)."""
+    ip = 2.0 if math.isinf(p) else p
+    rp = 1.0 if p == 1 else 2.0
+    Ci = np_cost(x, x, ip) if cost is None else cost
+    Cr = np_cost(x, x, rp) if cost is None else cost
+    winf = np_cost(x, x, p).max() if winf is None else winf
+    k = -1.0 / (eta_p * winf)
+    f = np.zeros(len(r)) if f0 is None else np.array(f0, np.float64)
+    done = 0
+    while True:
+        L = np_lse(Ci * k + f[None, :], 1)
+        res = np.abs(r - np.exp(f + L)).sum()
+        if res <= epsilon / 6 or done >= itermax:
+            break
+        f = 0.5 * (f + np.log(r) - L)
+        done += 1
+    P = np.exp(Cr * k + f[:, None] + f[None, :])
+    return f, np.abs(r - P.sum(1)).sum(), (P * Cr).sum(), done, winf
+
+
 def np_theta_update(theta0, res, c, eta_mu_i, eta_mu, adjust, minv, maxv):
     t = np.tanh((res - c) / eta_mu_i + 0.5 * (1 - eta_mu) * np.log((1 + theta0) / (1 - theta0)))
     return np.clip(t, minv, maxv) if adjust else t

@@ -85,7 +85,7 @@ def test_autograd_function_and_identity(oracle):
     s.backward()
     parts = sinkhorn_divergence(x, y, a, b, eps, 2.0, tol=1e-8)
     gx, _, ga, _ = divergence_grads(x, y, parts, 2.0)
-    assert abs(float(s) - parts.value) <= 1e-9 * max(1.0, abs(parts.value))
+    assert abs(float(s.detach()) - parts.value) <= 1e-9 * max(1.0, abs(parts.value))
     assert torch.allclose(xr.grad, gx, rtol=1e-6, atol=1e-12)
     assert torch.allclose(ar.grad, ga, rtol=1e-6, atol=1e-12)
     same = sinkhorn_divergence(x, x, a, a, eps, 2.0, tol=1e-8)

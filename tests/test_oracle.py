@@ -145,3 +145,22 @@ def test_bf16_split_emulation(oracle):
     assert 1e-7 < e3 < 2e-5 and e6 < 1e-8
     c = oracle.feature_cost(x, y)
     assert np.allclose(c, ((x[:, None, :] - y[None, :, :]) ** 2).sum(-1), rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("p", [1.0, 2.0])
+def test_symmetric_iteration_reaches_the_sinkhorn_fixed_point(oracle, p):
+    """The averaged symmetric iteration (self-transport terms of the Sinkhorn
+    divergence) converges to the alternating Sinkhorn solution: its f equals
+    (phi + psi)/2 of the alternating fixed point, and the two OT values agree."""
+    x, _, _, _ = D.rgb_instance(200, 200)
+    r = D.uniform_marginal(200, seed=3)
+    eta = 5e-2
+    f, res, cost, done, winf = oracle.np_symmetric_sinkhorn(x, r, eta, 500, epsilon=6e-12, p=p)
+    assert res <= 1e-12 and 0 < done < 100
+    phi, psi, res2, cost2, it, _ = oracle.np_sinkhorn_kernel(x, x, r, r, eta, 50000, 1, 6e-12, p)
+    assert res2 <= 1e-12 and it > 3 * done
+    np.testing.assert_allclose(f, 0.5 * (phi + psi), rtol=0, atol=1e-9)
+    ot_sym = eta * winf * 2 * np.dot(r, f)
+    ot_alt = eta * winf * (np.dot(r, phi) + np.dot(r, psi))
+    assert ot_sym == pytest.approx(ot_alt, rel=1e-9)
+    assert cost == pytest.approx(cost2, rel=1e-8)
