@@ -526,6 +526,16 @@ def extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_chosen, chosen_ms):
     gap = (l5.log[-1][4] - l5.log[-1][5]) if l5.log else float("nan")
     ex["lamp_65536"] = {"reached_tol": l5.stopped == 1, "ms": l5.elapsed_ms, "iterations": l5.iterations,
                         "residual": l5.residual, "gap": gap, "stop_rule": "gap and marginal"}
+    # the plain FP32 form of the same LAMP solve (same stopping rule, capped at
+    # twice the chosen form's iterations and 30 s)
+    pl5 = cb.solve_lamp(X5, Y5, R5, C5, bl.copy(itermax=2 * max(1, l5.iterations), tmax=30.0), 25, P,
+                        flags=cb.FLAG_CHECK_ALWAYS | cb.FLAG_FORM_PLAIN)
+    ex["plain_fp32_lamp_65536"] = {
+        "reached_tol": pl5.stopped == 1, "ms": pl5.elapsed_ms, "iterations": pl5.iterations,
+        "ms_per_iter": pl5.elapsed_ms / max(1, pl5.iterations),
+        "chosen_over_plain_speedup": (pl5.elapsed_ms / l5.elapsed_ms) if pl5.stopped == 1 else None,
+        "chosen_over_plain_per_iter": (pl5.elapsed_ms / max(1, pl5.iterations)) /
+                                      (l5.elapsed_ms / max(1, l5.iterations))}
     ex["features_16384_d256"] = feature_extra(cb, D, torch, dev)
     ex["divergence_65536"] = divergence_extra(cb, D, torch, dev, X5, Y5, R5, C5, s5.winf)
     return ex
@@ -641,12 +651,24 @@ def feature_extra(cb, D, torch, dev, n=16384, d=256):
     iteration over 20 iterations (two passes of 2*d*n*m useful FLOPs each), its
     fraction of the tensor roofline (measured bf16 peak / products per useful
     MAC), and a solve to 1e-6 L1 marginal error with the FP64-checked errors."""
+    from culamp_b200 import kernels as K
     x, y, r, c = D.feature_instance(n, n, d)
     X, Y, R, Cc = (torch.as_tensor(v, device=dev) for v in (x, y, r, c))
     peaks = load_peaks() or {}
     peak = peaks.get("bf16_tflops") or 1590.0
     out = {"n": n, "m": n, "d": d, "eta_p": 1e-2, "peak_bf16_tflops": peak,
            "peak_source": "MEASURED_PEAKS.json bf16_tflops" if "bf16_tflops" in peaks else "fallback"}
+    # W_inf (exact FP64 maximum over all pairs, once per solve): the register-
+    # tiled pass against the row-per-thread max pass, CUDA events, third call
+    for rows in (False, True):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        for _ in range(3):
+            ev[0].record()
+            _, w = K.max_logsumexp_spp_ct(X, Y, 2.0, rows=rows)
+            ev[1].record()
+        ev[1].synchronize()
+        out["winf_rowpass_ms" if rows else "winf_tiled_ms"] = ev[0].elapsed_time(ev[1])
+    out["winf_tiled_fp64_tflops"] = 2.0 * 2.0 * d * n * n / (out["winf_tiled_ms"] * 1e-3) / 1e12
     useful = 2.0 * 2.0 * d * n * n      # FLOPs of the two inner-product passes of one iteration
     for name, flag, prods in (("bf16x3", 0, 3), ("bf16x6", cb.FLAG_FEAT_X6, 6)):
         a = cb.EOTArgs(eta_p=1e-2, epsilon=0.0, itermax=20, tmax=60.0, verbose=False)

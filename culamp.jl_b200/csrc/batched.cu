@@ -117,7 +117,8 @@ struct Plan {
 
 struct culamp_handle_s::Batch {
     DevBuf X, Y, r, c, phi, psi, ctl, ctl2, part, tickets, blk, fx, fy, fxn, fyn, plist, tables, err,
-        pairs, active;
+        pairs, active, mctab;
+    std::vector<unsigned char> mctab_host;   // W_inf job table as uploaded
     cudaStream_t cap_stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<unsigned long long> tuned_sig;
@@ -125,7 +126,7 @@ struct culamp_handle_s::Batch {
 
     void release() {
         DevBuf *all[] = {&X, &Y, &r, &c, &phi, &psi, &ctl, &ctl2, &part, &tickets, &blk, &fx, &fy,
-                         &fxn, &fyn, &plist, &tables, &err, &pairs, &active};
+                         &fxn, &fyn, &plist, &tables, &err, &pairs, &active, &mctab};
         for (DevBuf *b : all) b->release();
         if (cap_stream) cudaStreamDestroy(cap_stream);
         if (ev0) cudaEventDestroy(ev0);
@@ -399,23 +400,14 @@ int reset_state(const Ctx &X, const culamp_args *args, int64_t frequency, cudaSt
     BT_TRY(h, cudaMemsetAsync(B.phi.ptr, 0, B.phi.bytes, st));
     BT_TRY(h, cudaMemsetAsync(B.psi.ptr, 0, B.psi.bytes, st));
     BT_TRY(h, cudaMemsetAsync(B.err.ptr, 0, sizeof(int), st));
+    // W_inf of every instance in one launch (the control blocks hold winf = +0)
+    std::vector<MaxCostInput> mc(X.count);
     for (int i = 0; i < X.count; ++i) {
         const Inst &I = X.in[i];
-        PassParams P;
-        std::memset(&P, 0, sizeof(P));
-        P.X = B.X.as<double>() + I.xo;
-        P.Y = B.Y.as<double>() + I.yo;
-        P.n = I.n;
-        P.m = I.m;
-        P.d = I.d;
-        P.pexp = X.p_true;
-        P.ctl = B.ctl.as<Ctl>() + i;
-        P.epi = EPI_RAW;
-        P.finish = FIN_MAXCOST;
-        const LaunchShape sh = pass_shape(I.n, I.m, I.d, ACC_MAX, h->sm_count);
-        BT_TRY(h, launch_pass_at(P, pmode_of(X.p_true), ACC_MAX, sh, B.part.as<double>() + I.parto,
-                                 B.tickets.as<unsigned>() + I.ticko, B.blk.as<double>() + I.blko, st));
+        mc[i] = {B.X.as<double>() + I.xo, B.Y.as<double>() + I.yo, I.n, I.m, I.d, &(B.ctl.as<Ctl>() + i)->winf};
     }
+    BT_TRY(h, B.mctab.reserve(max_cost_table_bytes(X.count)));
+    BT_TRY(h, launch_max_cost_batched(mc.data(), X.count, X.p_true, B.mctab.ptr, B.mctab_host, h->sm_count, st));
     batch_start_kernel<<<(X.count + 255) / 256, 256, 0, st>>>(B.ctl.as<Ctl>(), X.count);
     BT_TRY(h, cudaGetLastError());
     return CULAMP_OK;
@@ -648,6 +640,8 @@ extern "C" int culamp_batched_sinkhorn(culamp_handle h, const culamp_instance *i
         B.tuned_tpsm = tpsm;
         B.tuned_tpu = tpu;
     }
+    // device time from here: W_inf passes, then the solve loop
+    BT_TRY(h, cudaEventRecord(B.ev0, st));
     int s = reset_state(X, args, frequency, st);
     if (s) return s;
 
@@ -657,7 +651,6 @@ extern "C" int culamp_batched_sinkhorn(culamp_handle h, const culamp_instance *i
     std::vector<int> act = all;
     std::vector<Ctl> cs(count);
     int launches = 0, unroll = 1, phases = 0;
-    BT_TRY(h, cudaEventRecord(B.ev0, st));
     while (!act.empty()) {
         double apairs = 0.0;
         for (int i : act) apairs += pairs[i];

@@ -265,13 +265,20 @@ extern "C" int culamp_max_cost(culamp_handle h, const double *x, const double *y
     int s = check_common(h, x, y, n, m, d, p);
     if (s) return s;
     cudaStream_t st = (cudaStream_t)stream;
-    PassParams P = base_params(x, y, (int)n, (int)m, d, p);
-    P.epi = EPI_RAW;
-    P.out = rowmax;
-    P.ctl = h->pass_ctl.as<Ctl>();
-    P.finish = FIN_MAXCOST;
-    s = run_pass(h, P, pmode_of(p), ACC_MAX, st);
-    if (s) return s;
+    if (!rowmax) {
+        // W_inf alone: the register-tiled maximum (same per-pair costs)
+        double *dst = &h->pass_ctl.as<Ctl>()->winf;
+        CUDA_TRY(h, cudaMemsetAsync(dst, 0, sizeof(double), st));
+        CUDA_TRY(h, launch_max_cost(x, y, (int)n, (int)m, d, p, dst, h->sm_count, st));
+    } else {
+        PassParams P = base_params(x, y, (int)n, (int)m, d, p);
+        P.epi = EPI_RAW;
+        P.out = rowmax;
+        P.ctl = h->pass_ctl.as<Ctl>();
+        P.finish = FIN_MAXCOST;
+        s = run_pass(h, P, pmode_of(p), ACC_MAX, st);
+        if (s) return s;
+    }
     if (winf_host) {
         CUDA_TRY(h, cudaMemcpyAsync(winf_host, &h->pass_ctl.as<Ctl>()->winf, sizeof(double),
                                     cudaMemcpyDeviceToHost, st));

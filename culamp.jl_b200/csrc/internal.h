@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <vector>
 
 #include "../../include/culamp.h"
 #include "engine.cuh"
@@ -80,6 +81,22 @@ cudaError_t launch_pass_at(PassParams P, int pmode, int acc, const LaunchShape &
                            unsigned *tickets, double *blk, cudaStream_t st);
 
 int pmode_of(double p);   // P_L1 / P_SQ / P_INF / P_GEN
+
+// ---- W_inf = max_ij C(x_i, y_j) (maxcost.cu): exact FP64, register-tiled.
+// `dst` must hold +0.0 before the launch (the kernel folds in with atomicMax).
+cudaError_t launch_max_cost(const double *X, const double *Y, int n, int m, int d, double p,
+                            double *dst, int sm_count, cudaStream_t st);
+struct MaxCostInput {
+    const double *X, *Y;
+    int n, m, d;
+    double *dst;
+};
+// Device table bytes for `count` jobs; one launch over all of them. host_table
+// keeps the uploaded table alive until the copy has been consumed.
+size_t max_cost_table_bytes(int count);
+cudaError_t launch_max_cost_batched(const MaxCostInput *in, int count, double p, void *table,
+                                    std::vector<unsigned char> &host_table, int sm_count,
+                                    cudaStream_t st);
 
 // ---- feature-cost path (feature.cu): p = 2, d >= FEAT_MIN_D, tensor cores
 constexpr int FEAT_MIN_D = 32;

@@ -369,12 +369,10 @@ PassParams mk(const double *X, const double *Y, int n, int m, int d, double p, C
 // W_inf = max_ij C_ij with the solver's true p (MirrorProxKernel.jl:280-326).
 int compute_winf(culamp_handle h, int n, int m, int d, double p, cudaStream_t st, double *winf) {
     Solver &S = *h->solver;
-    PassParams P = mk(S.X.as<double>(), S.Y.as<double>(), n, m, d, p, h->pass_ctl.as<Ctl>());
-    P.epi = EPI_RAW;
-    P.finish = FIN_MAXCOST;
-    LaunchShape sh = pass_shape(n, m, d, ACC_MAX, h->sm_count);
-    CUDA_TRY(h, launch_pass(P, pmode_of(p), ACC_MAX, sh, S.scr, st));
-    CUDA_TRY(h, cudaMemcpyAsync(winf, &h->pass_ctl.as<Ctl>()->winf, sizeof(double), cudaMemcpyDeviceToHost, st));
+    double *dst = &h->pass_ctl.as<Ctl>()->winf;
+    CUDA_TRY(h, cudaMemsetAsync(dst, 0, sizeof(double), st));
+    CUDA_TRY(h, launch_max_cost(S.X.as<double>(), S.Y.as<double>(), n, m, d, p, dst, h->sm_count, st));
+    CUDA_TRY(h, cudaMemcpyAsync(winf, dst, sizeof(double), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(h, cudaStreamSynchronize(st));
     return CULAMP_OK;
 }

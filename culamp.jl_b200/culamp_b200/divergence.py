@@ -51,7 +51,7 @@ class OTResult:
 def entropic_ot(x, y, a, b, eps: float, p: float = 2.0, tol: float = 1e-7, frequency: int = 10,
                 itermax: int = 200_000, phi0=None, psi0=None) -> OTResult:
     """Kernel Sinkhorn at absolute regularisation eps, to L1 marginal error tol."""
-    _, winf = K.max_logsumexp_spp_ct(x, y, p)
+    _, winf = K.max_logsumexp_spp_ct(x, y, p, rows=False)
     eta_p = eps / winf
     args = EOTArgs(eta_p=eta_p, epsilon=6.0 * tol, itermax=itermax, verbose=False)
     res = solve_sinkhorn(x, y, a, b, args, frequency, p, phi0=phi0, psi0=psi0)
@@ -62,7 +62,7 @@ def entropic_ot(x, y, a, b, eps: float, p: float = 2.0, tol: float = 1e-7, frequ
 def entropic_ot_self(x, a, eps: float, p: float = 2.0, tol: float = 1e-7, frequency: int = 10,
                      itermax: int = 200_000, f0=None) -> OTResult:
     """OT_eps(a, a; x, x) by the symmetric iteration, to L1 marginal error tol."""
-    _, winf = K.max_logsumexp_spp_ct(x, x, p)
+    _, winf = K.max_logsumexp_spp_ct(x, x, p, rows=False)
     eta_p = eps / winf
     args = EOTArgs(eta_p=eta_p, epsilon=6.0 * tol, itermax=itermax, verbose=False)
     res = solve_symmetric_sinkhorn(x, a, args, frequency, p, f0=f0)

@@ -21,16 +21,17 @@ def _empty(n, like):
     return torch.empty(n, dtype=torch.float64, device=like.device)
 
 
-def max_logsumexp_spp_ct(x, y, p):
+def max_logsumexp_spp_ct(x, y, p, rows: bool = True):
     """MirrorProxKernel.jl:280-326 + `maximum` (SinkhornKernel.jl:500-502):
-    returns (rowmax, W_inf)."""
+    returns (rowmax, W_inf); with rows=False only W_inf is formed (rowmax None)."""
     n, d = x.shape
     m = y.shape[0]
-    out = _empty(n, x)
+    out = _empty(n, x) if rows else None
     w = C.c_double()
     h = _h(x)
     h.check(h._lib.culamp_max_cost(h.ptr, _dev(x, "x"), _dev(y, "y"), n, m, d, float(p),
-                                   C.c_void_p(out.data_ptr()), C.byref(w), _stream()),
+                                   C.c_void_p(out.data_ptr()) if rows else None, C.byref(w),
+                                   _stream()),
             "culamp_max_cost")
     return out, w.value
 

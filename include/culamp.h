@@ -109,7 +109,9 @@ int culamp_args_from_json_string(const char *json, culamp_args *out);
 
 /* max_logsumexp_spp_ct! (MirrorProxKernel.jl:280-326): rowmax[i] = max_j C(x_i, y_j)
  * (rowmax may be NULL); *winf_host (may be NULL) receives max_i rowmax[i]
- * (SinkhornKernel.jl:500-502) -- this one call synchronises the stream. */
+ * (SinkhornKernel.jl:500-502) -- this one call synchronises the stream. With
+ * rowmax NULL only W_inf is formed, by a register-tiled pass over 64 x 64 pair
+ * tiles (same value bit for bit). */
 int culamp_max_cost(culamp_handle h, const double *x, const double *y, int64_t n, int64_t m,
                     int32_t d, double p, double *rowmax, double *winf_host, void *stream);
 
@@ -267,7 +269,7 @@ typedef struct culamp_batch_stats {
 } culamp_batch_stats;
 
 typedef struct culamp_batch_info {
-    double elapsed_ms;    /* device time of the solve loop (one graph launch)          */
+    double elapsed_ms;    /* device time of the W_inf passes and the solve loop        */
     double tune_ms;       /* device time spent timing shape candidates (0 when cached) */
     int32_t target_ctas_per_sm;   /* chosen pair-pass shape: CTAs per SM over the batch */
     int32_t feat_tiles_per_unit;  /* chosen feature-pass work-unit size (column tiles)  */
