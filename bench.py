@@ -668,7 +668,8 @@ def feature_extra(cb, D, torch, dev, n=16384, d=256):
             ev[1].record()
         ev[1].synchronize()
         out["winf_rowpass_ms" if rows else "winf_tiled_ms"] = ev[0].elapsed_time(ev[1])
-    out["winf_tiled_fp64_tflops"] = 2.0 * 2.0 * d * n * n / (out["winf_tiled_ms"] * 1e-3) / 1e12
+    # one DSUB and one DFMA per pair and coordinate
+    out["winf_tiled_fp64_tinstr_s"] = 2.0 * d * n * n / (out["winf_tiled_ms"] * 1e-3) / 1e12
     useful = 2.0 * 2.0 * d * n * n      # FLOPs of the two inner-product passes of one iteration
     for name, flag, prods in (("bf16x3", 0, 3), ("bf16x6", cb.FLAG_FEAT_X6, 6)):
         a = cb.EOTArgs(eta_p=1e-2, epsilon=0.0, itermax=20, tmax=60.0, verbose=False)
