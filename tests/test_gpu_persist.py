@@ -1,0 +1,110 @@
+"""Whole Sinkhorn loop in one cooperative launch (persist.cu): p = 2 (and the
+p = Inf default, which iterates on the squared cost), d <= 3, n, m <= 6144
+take it by default; CULAMP_FLAG_NO_PERSIST runs the pass-per-launch path.
+Parity as for every solver path: potentials against the FP64 oracle after a
+fixed number of iterations (1e-5 of max(1, max |phi|), gauge-fixed within
+5e-6); at a tolerance the residual crosses decisively, the same stopping
+iteration, num_iter and check iterations as the pass path and the oracle;
+ragged shapes (row groups of 32 and 16 column slices cut by n and m), n != m,
+d = 1, 2, 3, and the size limit. Residual, objective and dual values in the
+log sum FP32 partials in another order than the pass path: they agree to
+rounding (~1e-7 relative), not bit for bit."""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def T(a):
+    import torch
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device="cuda")
+
+
+def gauge(v, w):
+    v = np.asarray(v, dtype=np.float64)
+    return v - np.dot(w, v) / np.sum(w)
+
+
+def cloud(n, m, d, seed):
+    from culamp_b200 import datasets as D
+    g = np.random.Generator(np.random.PCG64(seed))
+    return (g.uniform(size=(n, d)), g.uniform(size=(m, d)) + 0.1,
+            D.uniform_marginal(n, seed=seed + 1), D.uniform_marginal(m, seed=seed + 2))
+
+
+@pytest.mark.parametrize("n,m,d", [(1000, 777, 3), (33, 1500, 2), (1200, 31, 1), (1, 17, 2),
+                                   (517, 517, 3)])
+@pytest.mark.parametrize("p", [2.0, math.inf])
+def test_fixed_iterations_match_oracle(oracle, n, m, d, p):
+    import culamp_b200 as cb
+    x, y, r, c = cloud(n, m, d, n + m + d)
+    its = 40
+    a = cb.EOTArgs(eta_p=5e-3, epsilon=0.0, itermax=its, verbose=False)
+    res = cb.solve_sinkhorn(T(x), T(y), T(r), T(c), a, frequency=7, p=p)
+    assert res.iterations == its and res.stopped == 2
+    phi, psi, resid, cost, _, winf = oracle.np_sinkhorn_kernel(x, y, r, c, 5e-3, its, frequency=7, p=p)
+    assert res.winf == winf
+    for got, want, w in ((res.phi, phi, r), (res.psi, psi, c)):
+        got = got.cpu().numpy()
+        assert np.abs(got - want).max() <= 1e-5 * max(1.0, np.abs(want).max())
+        np.testing.assert_allclose(gauge(got, w), gauge(want, w), atol=5e-6, rtol=0)
+    assert res.objective == pytest.approx(cost, rel=1e-5)
+
+
+@pytest.mark.parametrize("freq", [1, 10])
+def test_stop_num_iter_and_log_match_pass_path(oracle, freq):
+    import culamp_b200 as cb
+    x, y, r, c = cloud(2048, 1900, 3, 5)
+    dev = [T(v) for v in (x, y, r, c)]
+    a = cb.EOTArgs(eta_p=5e-3, epsilon=6e-4, itermax=5000, verbose=True)
+    per = cb.solve_sinkhorn(*dev, a, frequency=freq, p=2.0)
+    ref = cb.solve_sinkhorn(*dev, a, frequency=freq, p=2.0, flags=cb.FLAG_NO_PERSIST)
+    assert per.stopped == ref.stopped == 1
+    assert (per.iterations, per.num_iter) == (ref.iterations, ref.num_iter)
+    lp, lr = np.array(per.log), np.array(ref.log)
+    assert lp.shape == lr.shape
+    assert np.array_equal(lp[:, 1], lr[:, 1])                                # check iterations
+    np.testing.assert_allclose(lp[:, 2], lr[:, 2], rtol=0, atol=2e-7)       # L1 residual
+    np.testing.assert_allclose(lp[:, 3], lr[:, 3], rtol=1e-5)               # transport cost
+    np.testing.assert_allclose(lp[:, 5], lr[:, 5], rtol=1e-5)               # dual value
+    np.testing.assert_allclose(gauge(per.phi.cpu().numpy(), r), gauge(ref.phi.cpu().numpy(), r),
+                               atol=5e-6, rtol=0)
+    xs, ys = x[:400], y[:400]
+    rs, cs = r[:400] / r[:400].sum(), c[:400] / c[:400].sum()
+    *_, it_o, _ = oracle.np_sinkhorn_kernel(xs, ys, rs, cs, 5e-3, 5000, freq, 6e-4)
+    sub = cb.solve_sinkhorn(T(xs), T(ys), T(rs), T(cs), a, frequency=freq, p=2.0)
+    assert sub.iterations == it_o
+
+
+def test_headline_shape_to_1e6_matches_pass_path():
+    """The 64 x 64 grid, eta_p = 1e-3, to 1e-6: the slow tail of the residual
+    lets rounding move the stop by a few checks, so iterations within 2 %; the
+    marginals re-evaluated in FP64 meet the tolerance."""
+    import culamp_b200 as cb
+    import bench
+    x, y, r, c = bench.instance()
+    dev = [T(v) for v in (x, y, r, c)]
+    a = cb.EOTArgs(eta_p=1e-3, epsilon=6e-6, itermax=200_000, verbose=False)
+    per = cb.solve_sinkhorn(*dev, a, frequency=10, p=2.0)
+    ref = cb.solve_sinkhorn(*dev, a, frequency=10, p=2.0, flags=cb.FLAG_NO_PERSIST)
+    assert per.stopped == ref.stopped == 1
+    assert abs(per.iterations - ref.iterations) <= 0.02 * ref.iterations + 10
+    assert per.residual <= 1e-6 * 1.05
+    rl, cl = cb.marginal_error_fp64(*dev, per.phi, per.psi, 1e-3, per.winf, 2.0)
+    assert rl <= 1.2e-6 and cl <= 1e-6
+
+
+def test_size_limit_and_other_costs_use_the_pass_path(oracle):
+    """n = 6145 and p = 1 take the pass path; it matches the oracle."""
+    import culamp_b200 as cb
+    x, y, r, c = cloud(6145, 300, 2, 8)
+    a = cb.EOTArgs(eta_p=1e-2, epsilon=0.0, itermax=5, verbose=False)
+    big = cb.solve_sinkhorn(T(x), T(y), T(r), T(c), a, frequency=5, p=2.0)
+    ref = cb.solve_sinkhorn(T(x), T(y), T(r), T(c), a, frequency=5, p=2.0, flags=cb.FLAG_NO_PERSIST)
+    assert np.array_equal(big.phi.cpu().numpy(), ref.phi.cpu().numpy())
+    x, y, r, c = cloud(300, 200, 3, 9)
+    one = cb.solve_sinkhorn(T(x), T(y), T(r), T(c), a, frequency=5, p=1.0)
+    phi, *_ = oracle.np_sinkhorn_kernel(x, y, r, c, 1e-2, 5, frequency=5, p=1.0)
+    np.testing.assert_allclose(gauge(one.phi.cpu().numpy(), r), gauge(phi, r), atol=5e-6, rtol=0)
