@@ -41,10 +41,7 @@ struct PersistArgs {
     const double *r, *c;       // marginals
     double *phi, *psi;         // potentials (phi / psi hold the starting point)
     Ctl *ctl;                  // control block (initialised, t_start set)
-    double *blk;               // [gridDim.x][4] per-CTA sums of the column pass
-    double *blk2;              // [gridDim.x][4] per-CTA sums of the check pass: a CTA
-                               // writes these right after reading blk, with no barrier
-                               // between, so the two must not share memory
+    double *blk;               // [gridDim.x][4] per-CTA partial sums
     unsigned *bar;             // [0] arrivals, [1] generation (zero before the launch)
     unsigned long long *tstamp;// CTA 0's clock for the iteration's tmax test
     int *err;                  // set when a barrier wait gave up
@@ -171,14 +168,14 @@ __device__ __forceinline__ void ps_pass(const double *Xr, int nr, const double *
 
 // Publish this CTA's sums, pass the barrier, and total every CTA's sums in CTA
 // order (the same totals in every CTA).
-__device__ __forceinline__ bool ps_totals(const PersistArgs &A, double *blk, const double (&acc)[4],
-                                          double (&tot)[4], int *s_ok) {
+__device__ __forceinline__ bool ps_totals(const PersistArgs &A, const double (&acc)[4], double (&tot)[4],
+                                          int *s_ok) {
     if (threadIdx.x == 0)
-        for (int k = 0; k < 4; ++k) blk[blockIdx.x * 4 + k] = acc[k];
+        for (int k = 0; k < 4; ++k) A.blk[blockIdx.x * 4 + k] = acc[k];
     if (!ps_sync(A, s_ok)) return false;
     for (int k = 0; k < 4; ++k) tot[k] = 0.0;
     for (unsigned b = 0; b < gridDim.x; ++b)
-        for (int k = 0; k < 4; ++k) tot[k] += __ldcg(blk + b * 4 + k);
+        for (int k = 0; k < 4; ++k) tot[k] += __ldcg(A.blk + b * 4 + k);
     return true;
 }
 
@@ -210,7 +207,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1) sk_persistent_kernel(const __gr
         acc[0] = 0.0;
         ps_pass<D, PS_ROW>(A.Y, A.m, A.X, A.n, A.phi, nullptr, A.c, A.psi, ctr, a2, scol, sM, sS, sMO, acc);
         if (blockIdx.x == 0 && threadIdx.x == 0) *(volatile unsigned long long *)A.tstamp = globaltimer_ns();
-        if (!(alive = ps_totals(A, A.blk, acc, tot, &s_ok))) break;
+        if (!(alive = ps_totals(A, acc, tot, &s_ok))) break;
         if (threadIdx.x == 0) {
             Ctl *c = &sctl;
             const unsigned long long now = __ldcg(A.tstamp);
@@ -228,7 +225,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1) sk_persistent_kernel(const __gr
             // residual and transport cost at (phi, psi); tolerance test
             double acc2[4] = {0.0, 0.0, 0.0, 0.0};
             ps_pass<D, PS_RESID>(A.X, A.n, A.Y, A.m, A.psi, A.phi, A.r, nullptr, ctr, a2, scol, sM, sS, sMO, acc2);
-            if (!(alive = ps_totals(A, A.blk2, acc2, tot, &s_ok))) break;
+            if (!(alive = ps_totals(A, acc2, tot, &s_ok))) break;
             if (threadIdx.x == 0) run_finish(fin, tot);
             __syncthreads();
         }
@@ -246,7 +243,7 @@ namespace culamp_host {
 using culamp_dev::PersistArgs;
 
 size_t sk_persistent_scratch_bytes(int sm_count) {
-    return (size_t)sm_count * 8 * sizeof(double) + 64;
+    return (size_t)sm_count * 4 * sizeof(double) + 64;
 }
 
 template <int D>
@@ -283,7 +280,6 @@ cudaError_t launch_sk_persistent(const double *X, const double *Y, int n, int m,
     A.err = reinterpret_cast<int *>(sb + 8);
     A.tstamp = reinterpret_cast<unsigned long long *>(sb + 16);
     A.blk = reinterpret_cast<double *>(sb + 64);
-    A.blk2 = A.blk + (size_t)sm_count * 4;          // grid <= sm_count
     cudaError_t e = cudaMemsetAsync(sb, 0, 64, st);
     if (e != cudaSuccess) return e;
     switch (d) {
