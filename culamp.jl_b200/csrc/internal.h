@@ -82,15 +82,6 @@ cudaError_t launch_pass_at(PassParams P, int pmode, int acc, const LaunchShape &
 
 int pmode_of(double p);   // P_L1 / P_SQ / P_INF / P_GEN
 
-// ---- whole Sinkhorn loop in one cooperative launch (persist.cu): p = 2,
-// 1 <= d <= 3, n, m <= SK_PERSIST_MAX. *used = false (nothing launched) when
-// the problem or the device does not fit; the caller then runs the pass path.
-constexpr int SK_PERSIST_MAX = 6144;
-size_t sk_persistent_scratch_bytes(int sm_count);
-cudaError_t launch_sk_persistent(const double *X, const double *Y, int n, int m, int d, const double *r,
-                                 const double *c, double *phi, double *psi, Ctl *ctl, void *scratch,
-                                 int sm_count, cudaStream_t st, bool *used);
-
 // ---- W_inf = max_ij C(x_i, y_j) (maxcost.cu): exact FP64, register-tiled.
 // `dst` must hold +0.0 before the launch (the kernel folds in with atomicMax).
 cudaError_t launch_max_cost(const double *X, const double *Y, int n, int m, int d, double p,

@@ -81,7 +81,7 @@ struct culamp_handle_s::Solver {
     int n = 0, m = 0, d = 0;
     long long generation = 0;
     DevBuf X, Y, r, c, phi, psi, res, cost, logz, aux, nu, nub, theta, thetab, eta_mu, tmp, ctl,
-        logbuf, setup, ws_phi, ws_psi, prev_phi, prev_psi, pers;
+        logbuf, setup, ws_phi, ws_psi, prev_phi, prev_psi;
     DevBuf hx, hy;             // host-variant staging (device side)
     // feature-cost path: both clouds as bf16 pieces in the MMA tile image + norms
     DevBuf fx, fy, fxn, fyn;
@@ -103,7 +103,7 @@ struct culamp_handle_s::Solver {
         drop_graphs();
         DevBuf *all[] = {&X, &Y, &r, &c, &phi, &psi, &res, &cost, &logz, &aux, &nu, &nub, &theta,
                          &thetab, &eta_mu, &tmp, &ctl, &logbuf, &setup, &ws_phi, &ws_psi,
-                         &prev_phi, &prev_psi, &hx, &hy, &fx, &fy, &fxn, &fyn, &pers};
+                         &prev_phi, &prev_psi, &hx, &hy, &fx, &fy, &fxn, &fyn};
         for (DevBuf *b : all) b->release();
         scr.release();
         if (cap_stream) cudaStreamDestroy(cap_stream);
@@ -164,7 +164,6 @@ int ensure_solver(culamp_handle h, int n, int m, int d, int64_t log_cap, int fea
     R(S.cost, nm * sizeof(double));
     R(S.logz, nm * sizeof(double));
     R(S.aux, nm * sizeof(double));
-    R(S.pers, sk_persistent_scratch_bytes(h->sm_count));
     R(S.nu, nm * sizeof(double));
     R(S.nub, nm * sizeof(double));
     R(S.theta, nm * sizeof(double));
@@ -497,14 +496,7 @@ int sinkhorn_loop(culamp_handle h, int n, int m, int d, double p, double eta, do
         return iteration(s, with_check);
     };
     CUDA_TRY(h, cudaEventRecord(S.ev0, st));
-    bool persisted = false;
-    if (!(flags & CULAMP_FLAG_NO_PERSIST) && !S.feat_active && pl.pm_iter == P_SQ && pl.pm_resid == P_SQ)
-        CUDA_TRY(h, launch_sk_persistent(S.X.as<double>(), S.Y.as<double>(), n, m, d, S.r.as<double>(),
-                                         S.c.as<double>(), S.phi.as<double>(), S.psi.as<double>(),
-                                         S.ctl.as<Ctl>(), S.pers.ptr, h->sm_count, st, &persisted));
-    if (persisted) {
-        // the whole loop ran in the cooperative launch
-    } else if (flags & CULAMP_FLAG_NO_GRAPH) {
+    if (flags & CULAMP_FLAG_NO_GRAPH) {
         // host-driven loop: check the stop flag after every iteration
         for (long long it = 0; it < args->itermax + 2; ++it) {
             CUDA_TRY(h, iteration(st, true));

@@ -29,7 +29,6 @@ FLAG_FORM_PLAIN = 8
 FLAG_NO_GRAPH = 16
 FLAG_FEAT_X6 = 32
 FLAG_FEAT_FP64 = 64
-FLAG_NO_PERSIST = 128
 
 
 class CulampError(RuntimeError):

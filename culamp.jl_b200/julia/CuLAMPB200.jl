@@ -22,7 +22,6 @@ const CULAMP_FLAG_FORM_PLAIN = UInt32(8)
 const CULAMP_FLAG_NO_GRAPH = UInt32(16)
 const CULAMP_FLAG_FEAT_X6 = UInt32(32)
 const CULAMP_FLAG_FEAT_FP64 = UInt32(64)
-const CULAMP_FLAG_NO_PERSIST = UInt32(128)
 
 # struct culamp_args (EOTArgs, src/Utilities.jl:18-31)
 struct CArgs

@@ -56,9 +56,6 @@ extern "C" {
                                           instead of the default BF16x3 (2 pieces)          */
 #define CULAMP_FLAG_FEAT_FP64     64u  /* feature clouds on the FP64 pair loops instead of
                                           the tensor cores (exact inner products, slow)     */
-#define CULAMP_FLAG_NO_PERSIST   128u  /* Sinkhorn: run the pass-per-launch loop even where
-                                          the whole solve fits one cooperative launch
-                                          (p = 2, d <= 3, n, m <= 6144)                     */
 
 /* EOTArgs (src/Utilities.jl:18-31), same field names and defaults. */
 typedef struct culamp_args {
