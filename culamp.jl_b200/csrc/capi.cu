@@ -71,12 +71,14 @@ extern "C" int culamp_create(culamp_handle *out, int device) {
 
 void culamp_solver_release(culamp_handle h);   // solvers.cu
 void culamp_batch_release(culamp_handle h);    // batched.cu
+void culamp_dense_release(culamp_handle h);    // dense.cu
 
 extern "C" int culamp_destroy(culamp_handle h) {
     if (!h) return CULAMP_ERR_INVALID_ARG;
     cudaSetDevice(h->device);
     culamp_solver_release(h);
     culamp_batch_release(h);
+    culamp_dense_release(h);
     h->scratch.release();
     h->pass_ctl.release();
     h->tmpA.release();

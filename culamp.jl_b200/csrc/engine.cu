@@ -1,6 +1,6 @@
-// engine.cu -- template instantiations of the pair-pass kernel and the launcher.
+// engine.cu -- launch shape of the pair passes and the launch dispatch.
 #include <cmath>
-
+#include <cstdlib>
 #include <cstring>
 
 #include "internal.h"
@@ -8,6 +8,16 @@
 namespace culamp_host {
 
 using namespace culamp_dev;
+
+static thread_local int t_pdl_off = 0;
+
+bool pdl_launches() {
+    static const bool on = std::getenv("CULAMP_NO_PDL") == nullptr;
+    return on && t_pdl_off == 0;
+}
+
+PdlOff::PdlOff() { ++t_pdl_off; }
+PdlOff::~PdlOff() { --t_pdl_off; }
 
 int pmode_of(double p) {
     if (p == 1.0) return P_L1;
@@ -66,97 +76,20 @@ LaunchShape pass_shape(int n, int m, int d, int acc, int sm_count, bool mom) {
     return s;
 }
 
-template <int PM, int D, int ACC, int R, bool MOM, bool FR = false>
-static cudaError_t launch_t(const PassParams &P, const LaunchShape &sh, cudaStream_t st) {
-    auto kern = pair_pass_kernel<PM, D, ACC, R, MOM, FR>;
-    if (sh.smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)sh.smem);
-        if (e != cudaSuccess) return e;
-    }
-    dim3 grid(sh.rb, sh.splits);
-    kern<<<grid, TPB, sh.smem, st>>>(P, nullptr, nullptr, 0);
-    return cudaGetLastError();
-}
+// Per-cost launchers (engine_p1.cu, engine_p2.cu, engine_pinf.cu, engine_pgen.cu)
+// and the batched launcher (engine_bat.cu).
+cudaError_t launch_pair_l1(const PassParams &P, int acc, const LaunchShape &sh, cudaStream_t st);
+cudaError_t launch_pair_sq(const PassParams &P, int acc, const LaunchShape &sh, cudaStream_t st);
+cudaError_t launch_pair_inf(const PassParams &P, int acc, const LaunchShape &sh, cudaStream_t st);
+cudaError_t launch_pair_gen(const PassParams &P, int acc, const LaunchShape &sh, cudaStream_t st);
 
-template <int PM, int D, int ACC>
-static cudaError_t launch_v(const PassParams &P, const LaunchShape &sh, cudaStream_t st) {
-    if constexpr (ACC == ACC_LSE) {
-        if (P.want_moment) return launch_t<PM, D, ACC, RPT, true>(P, sh, st);
-        if constexpr (D > 0) {
-            if (P.use_ref) {
-                if (sh.R == RPT_BIG) return launch_t<PM, D, ACC, RPT_BIG, false, true>(P, sh, st);
-                if (sh.R == RPT_MID) return launch_t<PM, D, ACC, RPT_MID, false, true>(P, sh, st);
-                return launch_t<PM, D, ACC, RPT, false, true>(P, sh, st);
-            }
-            if (sh.R == RPT_BIG) return launch_t<PM, D, ACC, RPT_BIG, false>(P, sh, st);
-            if (sh.R == RPT_MID) return launch_t<PM, D, ACC, RPT_MID, false>(P, sh, st);
-        }
-    }
-    return launch_t<PM, D, ACC, RPT, false>(P, sh, st);
-}
-
-template <int PM, int ACC>
-static cudaError_t launch_d(const PassParams &P, const LaunchShape &sh, cudaStream_t st) {
-    switch (P.d) {
-        case 1: return launch_v<PM, 1, ACC>(P, sh, st);
-        case 2: return launch_v<PM, 2, ACC>(P, sh, st);
-        case 3: return launch_v<PM, 3, ACC>(P, sh, st);
-        default: return launch_v<PM, 0, ACC>(P, sh, st);
-    }
-}
-
-template <int ACC>
-static cudaError_t launch_p(const PassParams &P, int pm, const LaunchShape &sh, cudaStream_t st) {
+static cudaError_t launch_any(const PassParams &P, int pm, int acc, const LaunchShape &sh, cudaStream_t st) {
     switch (pm) {
-        case P_L1: return launch_d<P_L1, ACC>(P, sh, st);
-        case P_SQ: return launch_d<P_SQ, ACC>(P, sh, st);
-        case P_INF: return launch_d<P_INF, ACC>(P, sh, st);
-        default: return launch_d<P_GEN, ACC>(P, sh, st);
+        case P_L1: return launch_pair_l1(P, acc, sh, st);
+        case P_SQ: return launch_pair_sq(P, acc, sh, st);
+        case P_INF: return launch_pair_inf(P, acc, sh, st);
+        default: return launch_pair_gen(P, acc, sh, st);
     }
-}
-
-template <int PM, int D, bool MOM, bool FR>
-static cudaError_t launch_b(const PassParams *plist, const int *block_start, int count, int total_blocks,
-                            size_t smem, cudaStream_t st) {
-    auto kern = pair_pass_kernel<PM, D, ACC_LSE, RPT, MOM, FR, true>;
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    PassParams dummy;
-    memset(&dummy, 0, sizeof(dummy));
-    kern<<<total_blocks, TPB, smem, st>>>(dummy, plist, block_start, count);
-    return cudaGetLastError();
-}
-
-template <int PM, int D>
-static cudaError_t launch_bd(const PassParams *plist, const int *block_start, int count, int total_blocks,
-                             size_t smem, bool mom, bool fr, cudaStream_t st) {
-    if (mom) return launch_b<PM, D, true, false>(plist, block_start, count, total_blocks, smem, st);
-    if (fr && D > 0) return launch_b<PM, D, false, (D > 0)>(plist, block_start, count, total_blocks, smem, st);
-    return launch_b<PM, D, false, false>(plist, block_start, count, total_blocks, smem, st);
-}
-
-template <int PM>
-static cudaError_t launch_bp(const PassParams *plist, const int *block_start, int count, int total_blocks,
-                             size_t smem, int d, bool mom, bool fr, cudaStream_t st) {
-    switch (d) {
-        case 1: return launch_bd<PM, 1>(plist, block_start, count, total_blocks, smem, mom, fr, st);
-        case 2: return launch_bd<PM, 2>(plist, block_start, count, total_blocks, smem, mom, fr, st);
-        case 3: return launch_bd<PM, 3>(plist, block_start, count, total_blocks, smem, mom, fr, st);
-        default: return launch_bd<PM, 0>(plist, block_start, count, total_blocks, smem, mom, fr, st);
-    }
-}
-
-cudaError_t launch_pass_batched(const PassParams *plist, const int *block_start, int count,
-                                int total_blocks, size_t smem, int pm, int d, int acc, bool mom,
-                                bool fixed_ref, cudaStream_t st) {
-    if (count < 1 || total_blocks < 1) return cudaSuccess;
-    if (acc != ACC_LSE) return cudaErrorInvalidValue;
-    if (pm == P_SQ) return launch_bp<P_SQ>(plist, block_start, count, total_blocks, smem, d, mom, fixed_ref, st);
-    if (pm == P_L1) return launch_bp<P_L1>(plist, block_start, count, total_blocks, smem, d, mom, fixed_ref, st);
-    return cudaErrorNotSupported;
 }
 
 cudaError_t launch_pass_at(PassParams P, int pm, int acc, const LaunchShape &sh, double *part,
@@ -168,11 +101,7 @@ cudaError_t launch_pass_at(PassParams P, int pm, int acc, const LaunchShape &sh,
     P.rb_ticket = tickets;
     P.grid_ticket = tickets + sh.rb;
     P.blk = blk;
-    switch (acc) {
-        case ACC_LSE: return launch_p<ACC_LSE>(P, pm, sh, st);
-        case ACC_MAX: return launch_p<ACC_MAX>(P, pm, sh, st);
-        default: return launch_p<ACC_MIN>(P, pm, sh, st);
-    }
+    return launch_any(P, pm, acc, sh, st);
 }
 
 cudaError_t launch_pass(PassParams P, int pm, int acc, const LaunchShape &sh, Scratch &scr,
@@ -188,11 +117,7 @@ cudaError_t launch_pass(PassParams P, int pm, int acc, const LaunchShape &sh, Sc
     if (scr.part.bytes < sh.part_bytes || scr.tickets.bytes < (size_t)(sh.rb + 1) * sizeof(unsigned) ||
         scr.blk.bytes < (size_t)sh.rb * 4 * sizeof(double))
         return cudaErrorInvalidValue;
-    switch (acc) {
-        case ACC_LSE: return launch_p<ACC_LSE>(P, pm, sh, st);
-        case ACC_MAX: return launch_p<ACC_MAX>(P, pm, sh, st);
-        default: return launch_p<ACC_MIN>(P, pm, sh, st);
-    }
+    return launch_any(P, pm, acc, sh, st);
 }
 
 }  // namespace culamp_host

@@ -691,24 +691,57 @@ __device__ __forceinline__ void lse_step(const double4 col, const double (&xr)[R
 // x = t - Mref - 1, one DADD forms D = x + 1.5*2^20 (+2^-24 so the truncation
 // below rounds). D's ulp is 2^-32, so for |x| < 2^19 its high word carries
 // 2^19 + floor(x) in its low 20 bits and its low word is frac(x) * 2^32. Then
-//   * n = floor(x) is clamped to [-127, 126] by two 32-bit integer min/max on
-//     the high word (IEEE bit patterns are monotone in the value, so +-inf and
-//     out-of-range x clamp correctly);
+//   * k = floor(x) + FR_C0 is formed and clamped to [0, 126] by one integer
+//     add + min-with-relu on the high word (IEEE bit patterns are monotone in
+//     the value, so -inf and very negative x clamp to 0, +inf / NaN to 126);
 //   * a funnel shift of the low word under 0x7F gives v = 1 + frac(x) (23 bits);
-//   * 2^(t - Mref) = 2^(1 + x) = ex2(v) * 2^n: one MUFU ex2, and n is added to the
-//     exponent field as (hi << 23) (the 2^19 offset vanishes modulo 2^32).
+//   * ex2(v) lies in [2, 4) (exponent field 128); adding k to the exponent
+//     field gives e = 2^(1 + frac(x) + k) = 2^(t - Mref) * 2^FR_C0: every term
+//     is carried scaled by 2^FR_C0, exact for floor(x) in [-FR_C0, 126 - FR_C0],
+//     one MUFU ex2 per pair.
+// The terms of two rows (or, with one row per thread, of two columns) are
+// summed with one packed FP32x2 add.
 // No FP64->FP32 conversion, no FP64 min/max, no per-pair max test.
-// Clamped-low terms contribute < 2^-125 each. A column slice whose partial sum
-// exceeds 2^64 (a term clamped high, or a non-finite input) is recomputed by its
-// CTA with tile_lse_packed; after the slices are merged, a row whose full LSE
-// lies more than 61 (log2 units) below its reference -- where the clamped-low
-// terms could matter -- makes the merging CTA recompute its row block over all
-// columns the same way.
-constexpr double FR_LOW_MARGIN = 61.0;
+// A clamped-low term is carried as at most 4 (scaled), i.e. 2^(2 - FR_C0)
+// relative to the reference. A column slice whose scaled partial sum exceeds
+// 2^126 (a term clamped high, any term above the reference by >= 45, or a
+// non-finite input) is recomputed by its CTA with tile_lse_packed; after the
+// slices are merged, a row whose full LSE lies more than
+// FR_C0 - 32 - log2(m) below its reference -- where the m clamped-low terms
+// could reach 2^-30 of the row sum -- makes the merging CTA recompute its row
+// block over all columns the same way.
+constexpr int FR_C0 = 80;
+constexpr double FR_UNSCALE = 0x1p-80;             // 2^-FR_C0
+constexpr double FR_SUM_MAX = 0x1p126;             // largest accepted scaled partial sum
 constexpr double FR_MAGIC = 1572864.0 + 0x1p-24;   // 1.5 * 2^20, plus the rounding half-ulp
-constexpr int FR_H0 = 0x41380000;                  // high word of 1.5 * 2^20 (n = 0)
-constexpr int FR_HLO = FR_H0 - 127;
-constexpr int FR_HHI = FR_H0 + 126;
+constexpr int FR_H0 = 0x41380000;                  // high word of 1.5 * 2^20 (floor(x) = 0)
+constexpr int FR_KOFF = FR_C0 - FR_H0;             // high word + FR_KOFF = floor(x) + FR_C0
+
+__device__ __forceinline__ double fr_low_margin(int m) {
+    return (double)FR_C0 - 32.0 - log2((double)(m > 1 ? m : 1));
+}
+
+// k = clamp(hi + FR_KOFF, 0, 126): one add and one min-with-relu.
+__device__ __forceinline__ int fr_clamp_k(int hi) {
+    int k;
+    asm("{.reg .s32 t;\n\tadd.s32 t, %1, %2;\n\tmin.s32.relu %0, t, %3;}"
+        : "=r"(k) : "r"(hi), "n"(FR_KOFF), "n"(126));
+    return k;
+}
+
+// Packed FP32x2 add (sm_100): {a.lo + b.lo, a.hi + b.hi}.
+__device__ __forceinline__ unsigned long long add_f32x2(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long pack_f32x2(float lo, float hi) {
+    unsigned long long d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+    return d;
+}
+__device__ __forceinline__ float lo_f32(unsigned long long v) { return __uint_as_float((unsigned)v); }
+__device__ __forceinline__ float hi_f32(unsigned long long v) { return __uint_as_float((unsigned)(v >> 32)); }
 
 // The row's previous log-sum-exp (natural log), read from the buffer the
 // epilogue overwrites: phi -> log(marg) - phi, logZ -> logZ, column mass ->
@@ -722,9 +755,10 @@ __device__ __forceinline__ double row_reference(const PassParams &P, int o, doub
     return NAN;
 }
 
+// Scaled terms e[r] = 2^(t - Mref_r) * 2^FR_C0 of one column against R rows.
 template <int PM, int D, int R>
-__device__ __forceinline__ void fr_step(const double4 col, const double (&xr)[R][D], double a2,
-                                        double pexp, const double (&K)[R], float (&cs)[R]) {
+__device__ __forceinline__ void fr_terms(const double4 col, const double (&xr)[R][D], double a2,
+                                         double pexp, const double (&K)[R], float (&e)[R]) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         double t;
@@ -738,10 +772,56 @@ __device__ __forceinline__ void fr_step(const double4 col, const double (&xr)[R]
             t = fma(pair_cost_direct<PM>(xr[r], yv, D, pexp), a2, col.w);
         }
         const double dv = t + K[r];
-        const int hi = min(max(__double2hiint(dv), FR_HLO), FR_HHI);
+        const int k = fr_clamp_k(__double2hiint(dv));
         const float v = __int_as_float((int)__funnelshift_r((unsigned)__double2loint(dv), 0x7Fu, 9));
-        const float e = __int_as_float(__float_as_int(ex2_approx(v)) + (hi << 23));
-        cs[r] += e;
+        e[r] = __int_as_float(__float_as_int(ex2_approx(v)) + (k << 23));
+    }
+}
+
+// Packed accumulators: rows (2r, 2r+1) share one FP32x2 register; with one row
+// per thread, even and odd columns do.
+template <int R>
+struct FrAcc {
+    static constexpr int NP = (R + 1) / 2;
+    unsigned long long cs[NP];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int j = 0; j < NP; ++j) cs[j] = 0ull;
+    }
+    // R >= 2: one column's terms for all rows
+    __device__ __forceinline__ void add_rows(const float (&e)[R]) {
+#pragma unroll
+        for (int j = 0; j < R / 2; ++j) cs[j] = add_f32x2(cs[j], pack_f32x2(e[2 * j], e[2 * j + 1]));
+        if (R & 1) cs[NP - 1] = add_f32x2(cs[NP - 1], pack_f32x2(e[R - 1], 0.f));
+    }
+    // R == 1: the terms of two columns
+    __device__ __forceinline__ void add_cols(float e0, float e1) { cs[0] = add_f32x2(cs[0], pack_f32x2(e0, e1)); }
+    __device__ __forceinline__ float row(int r) const {
+        if (R == 1) return lo_f32(cs[0]) + hi_f32(cs[0]);
+        return (r & 1) ? hi_f32(cs[r >> 1]) : lo_f32(cs[r >> 1]);
+    }
+};
+
+template <int PM, int D, int R>
+__device__ __forceinline__ void fr_col(const double4 col, const double (&xr)[R][D], double a2,
+                                       double pexp, const double (&K)[R], FrAcc<R> &acc) {
+    float e[R];
+    fr_terms<PM, D, R>(col, xr, a2, pexp, K, e);
+    if constexpr (R == 1) acc.add_cols(e[0], 0.f);
+    else acc.add_rows(e);
+}
+
+template <int PM, int D, int R>
+__device__ __forceinline__ void fr_col2(const double4 c0, const double4 c1, const double (&xr)[R][D],
+                                        double a2, double pexp, const double (&K)[R], FrAcc<R> &acc) {
+    if constexpr (R == 1) {
+        float e0[1], e1[1];
+        fr_terms<PM, D, 1>(c0, xr, a2, pexp, K, e0);
+        fr_terms<PM, D, 1>(c1, xr, a2, pexp, K, e1);
+        acc.add_cols(e0[0], e1[0]);
+    } else {
+        fr_col<PM, D, R>(c0, xr, a2, pexp, K, acc);
+        fr_col<PM, D, R>(c1, xr, a2, pexp, K, acc);
     }
 }
 
@@ -760,7 +840,9 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
 #pragma unroll
     for (int k = 0; k < D; ++k) ctr[k] = P.ctr ? P.ctr[k] : 0.0;
     double xr[R][D], K[R];
-    float S[R], Cc[R], cs[R];
+    float S[R], Cc[R];
+    FrAcc<R> acc;
+    acc.zero();
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int row = row_base + tid + r * TPB;
@@ -774,7 +856,7 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
         }
         const double m = (ok ? row_reference(P, row, beta) * LOG2E : 0.0) - (SQ ? a2 * h : 0.0);
         K[r] = FR_MAGIC - (m + 1.0);
-        S[r] = 0.f; Cc[r] = 0.f; cs[r] = 0.f;
+        S[r] = 0.f; Cc[r] = 0.f;
     }
     double4 *tile = reinterpret_cast<double4 *>(smem);
     for (int c0 = cbeg; c0 < cend; c0 += CHUNK) {
@@ -801,20 +883,22 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
         const int nc = min(CHUNK, cend - c0);
         int q = 0;
         // few rows per thread (small problems): unroll more columns so each warp
-        // has enough independent pairs in flight to cover FP64 / MUFU latency
-        // 16 columns per FP32 chunk sum before the compensated merge: measured
-        // 2.5 % faster than 8 at 65536^2; a 16-term FP32 sum keeps a typical
-        // relative error near 2e-7 of the chunk
-        constexpr int FR_UNROLL = (R > RPT) ? 2 : 8;
+        // has enough independent pairs in flight to cover FP64 / MUFU latency.
+        // 16 columns per FP32 chunk sum before the compensated merge: a 16-term
+        // FP32 sum keeps a typical relative error near 2e-7 of the chunk
+        constexpr int FR_UNROLL = (R > RPT) ? 1 : 4;
         for (; q + 16 <= nc; q += 16) {
 #pragma unroll FR_UNROLL
-            for (int u = 0; u < 16; ++u) fr_step<PM, D, R>(tile[q + u], xr, a2, P.pexp, K, cs);
+            for (int u = 0; u < 16; u += 2)
+                fr_col2<PM, D, R>(tile[q + u], tile[q + u + 1], xr, a2, P.pexp, K, acc);
 #pragma unroll
-            for (int r = 0; r < R; ++r) { kahan_add(S[r], Cc[r], cs[r]); cs[r] = 0.f; }
+            for (int r = 0; r < R; ++r) kahan_add(S[r], Cc[r], acc.row(r));
+            acc.zero();
         }
-        for (; q < nc; ++q) fr_step<PM, D, R>(tile[q], xr, a2, P.pexp, K, cs);
+        for (; q < nc; ++q) fr_col<PM, D, R>(tile[q], xr, a2, P.pexp, K, acc);
 #pragma unroll
-        for (int r = 0; r < R; ++r) { kahan_add(S[r], Cc[r], cs[r]); cs[r] = 0.f; }
+        for (int r = 0; r < R; ++r) kahan_add(S[r], Cc[r], acc.row(r));
+        acc.zero();
     }
     bool good = true;
 #pragma unroll
@@ -830,10 +914,10 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
         Ho[r] = SQ ? a2 * h : 0.0;
         Mo[r] = (real_row ? row_reference(P, row, beta) * LOG2E : 0.0) - Ho[r];
         const double sv = (double)S[r] - (double)Cc[r];
-        So[r] = sv;
+        So[r] = sv * FR_UNSCALE;
         // this slice's partial sum must not hold a term clamped high; a small
         // partial is fine (the lower side is checked on the merged row)
-        if (real_row && !(sv <= 0x1p64)) good = false;
+        if (real_row && !(sv <= FR_SUM_MAX)) good = false;
     }
     return good;
 }
@@ -1052,6 +1136,11 @@ __global__ void __launch_bounds__(TPB, (R > RPT_MID) ? 3 : 4)
     __shared__ int s_last;
     __shared__ int s_bat[3];                      // BAT: row block, split, row-block count
     __shared__ __align__(16) PassParams sP;       // BAT: this instance's parameters
+    // Programmatic dependent launch: the launch may overlap the previous kernel
+    // in the stream, so before reading anything that kernel may write (control
+    // block, potentials, references, scratch) wait for it to complete. A no-op
+    // for a launch without programmatic serialisation.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     if constexpr (BAT) {
         if (threadIdx.x == 0) {
             int lo = 0, hi = count - 1;
@@ -1123,6 +1212,10 @@ __global__ void __launch_bounds__(TPB, (R > RPT_MID) ? 3 : 4)
         tile_reduce<PM, D, ACC, MOM>(P, alpha, beta, row_base, cbeg, cend, smem, Mv, Sv, MOMv, Hv);
     }
 
+    // the pair loop is done: let the next kernel in the stream start launching
+    // (it waits for this grid's completion before it reads anything)
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+
     if (P.splits > 1) {
         // publish partials, take a ticket; the last CTA of this row block merges
 #pragma unroll
@@ -1176,17 +1269,18 @@ __global__ void __launch_bounds__(TPB, (R > RPT_MID) ? 3 : 4)
 
     if constexpr (FR && ACC == ACC_LSE && D > 0 && !MOM) {
         // Lower side of the fixed-reference window, on the merged row: the full
-        // LSE must be within FR_LOW_MARGIN of the reference, else clamped-low
+        // LSE must be within fr_low_margin(m) of the reference, else clamped-low
         // terms could matter and the row block is recomputed over all columns.
         if (fr_tried) {
             const double a2 = alpha * LOG2E;
+            const double margin = fr_low_margin(P.m);
             bool bad = false;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int o = row_base + threadIdx.x + r * TPB;
                 if (o >= P.n) continue;
                 const double mref = row_reference(P, o, beta) * LOG2E - Hv[r];
-                if (!(Sv[r] > 0.0) || Mv[r] + log2(Sv[r]) < mref - FR_LOW_MARGIN) bad = true;
+                if (!(Sv[r] > 0.0) || Mv[r] + log2(Sv[r]) < mref - margin) bad = true;
             }
             (void)a2;
             if (__syncthreads_or(bad))

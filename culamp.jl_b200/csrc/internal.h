@@ -82,6 +82,17 @@ cudaError_t launch_pass_at(PassParams P, int pmode, int acc, const LaunchShape &
 
 int pmode_of(double p);   // P_L1 / P_SQ / P_INF / P_GEN
 
+// Whether pair passes launch with programmatic stream serialisation (PDL):
+// on unless CULAMP_NO_PDL is set in the environment (read once) or a PdlOff
+// guard is alive on this thread.
+bool pdl_launches();
+struct PdlOff {
+    PdlOff();
+    ~PdlOff();
+    PdlOff(const PdlOff &) = delete;
+    PdlOff &operator=(const PdlOff &) = delete;
+};
+
 // ---- W_inf = max_ij C(x_i, y_j) (maxcost.cu): exact FP64, register-tiled.
 // `dst` must hold +0.0 before the launch (the kernel folds in with atomicMax).
 cudaError_t launch_max_cost(const double *X, const double *Y, int n, int m, int d, double p,
@@ -148,6 +159,8 @@ struct culamp_handle_s {
     Solver *solver = nullptr;
     struct Batch;                      // batched-solve workspace, tuned shapes, graph
     Batch *batch = nullptr;
+    struct Dense;                      // dense-cost solver workspace (W^T, check rows)
+    Dense *dense = nullptr;
 };
 
 int culamp_set_error(culamp_handle h, int code, const char *fmt, ...);

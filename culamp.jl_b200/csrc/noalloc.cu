@@ -2,14 +2,10 @@
 // (warp_logsumexp_ct_fused!) with no device allocation at all.
 //
 // Who needs it. Some callers cannot let a library allocate device memory when
-// they call it:
-//  * code that records the call into a CUDA graph with stream capture --
-//    cudaMalloc is not a capturable operation, and an allocation made during
-//    capture would leave the graph holding a pointer the library may later
-//    free or move;
-//  * hosts that own every byte of device memory through their own pool or a
-//    fixed budget (serving runtimes, engines embedding the solver) and do not
-//    allow third-party cudaMalloc / cudaFree.
+// they call it: hosts that own every byte of device memory through their own
+// pool or a fixed budget (serving runtimes, engines that embed the solver next
+// to a model) and forbid third-party cudaMalloc / cudaFree, because an
+// allocation they did not plan for can fail or fragment their pool mid-run.
 // The handle-based culamp_lse_rows_sk grows its scratch with cudaMalloc on
 // demand, so it cannot serve them; this entry point takes no handle and uses
 // only the fixed scratch below.
@@ -19,9 +15,10 @@
 //   * g_noalloc_part: NOALLOC_PART_ENTRIES (split, row) partial results of three
 //     doubles each (3 MiB); when n * splits would exceed it the pass uses fewer
 //     column splits (a single split needs no partials at all);
-//   * g_noalloc_tickets: NOALLOC_TICKETS row-block tickets (256 KiB), which
-//     bounds n to (NOALLOC_TICKETS - 1) row blocks of at least 256 rows, i.e.
-//     n <= 16,777,216; larger n is rejected with CULAMP_ERR_UNSUPPORTED.
+//   * g_noalloc_tickets: NOALLOC_TICKETS row-block tickets (256 KiB). A row
+//     block holds at least 128 rows (one per thread), so n is limited to
+//     NOALLOC_MAX_ROWS = (NOALLOC_TICKETS - 1) * 128 = 8,388,608 rows for every
+//     d; larger n is rejected with CULAMP_ERR_UNSUPPORTED before any launch.
 // Every call shares these arrays and they keep the last call's contents: each
 // call clears the tickets it uses (cudaMemsetAsync, no allocation) before its
 // launch, and the partials are always written before they are read. Calls
@@ -32,6 +29,8 @@
 // arrays' device addresses with cudaGetSymbolAddress; a host-side name of a
 // __device__ array is only a stand-in and must never be passed to a kernel.
 // That first call may load the module, so make it before any stream capture.
+// A set-up that fails (CULAMP_ERR_CUDA) is not remembered: the next call on
+// that device tries again.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -43,30 +42,44 @@ namespace {
 constexpr int NOALLOC_PART_ENTRIES = 1 << 17;
 constexpr int NOALLOC_TICKETS = (1 << 16) + 1;
 constexpr int NOALLOC_MAX_DEVICES = 64;
+constexpr int64_t NOALLOC_MAX_ROWS = (int64_t)(NOALLOC_TICKETS - 1) * culamp_dev::TPB;
 
 __device__ __align__(256) double g_noalloc_part[3 * NOALLOC_PART_ENTRIES];
 __device__ __align__(256) unsigned int g_noalloc_tickets[NOALLOC_TICKETS];
 
 struct NoallocDevice {
-    std::once_flag once;
-    cudaError_t status = cudaSuccess;
+    bool ready = false;          // addresses resolved (set only on success)
     double *part = nullptr;
     unsigned int *tickets = nullptr;
     int sm_count = 0;
 };
 NoallocDevice g_devices[NOALLOC_MAX_DEVICES];
+std::mutex g_setup_mutex;
 
+// Resolves the device addresses of the fixed arrays for `dev` (current). On
+// failure nothing is recorded, so a later call retries the set-up.
 cudaError_t noalloc_setup(int dev, NoallocDevice **out) {
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
     NoallocDevice &d = g_devices[dev];
-    std::call_once(d.once, [&d, dev]() {
-        cudaError_t e = cudaGetSymbolAddress((void **)&d.part, g_noalloc_part);
-        if (e == cudaSuccess) e = cudaGetSymbolAddress((void **)&d.tickets, g_noalloc_tickets);
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, dev);
-        d.status = e;
-    });
+    if (!d.ready) {
+        double *part = nullptr;
+        unsigned int *tickets = nullptr;
+        int sms = 0;
+        cudaError_t e = cudaGetSymbolAddress((void **)&part, g_noalloc_part);
+        if (e == cudaSuccess) e = cudaGetSymbolAddress((void **)&tickets, g_noalloc_tickets);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) {
+            cudaGetLastError();   // clear it: the next call starts clean and retries
+            return e;
+        }
+        d.part = part;
+        d.tickets = tickets;
+        d.sm_count = sms;
+        d.ready = true;
+    }
     *out = &d;
-    return d.status;
+    return cudaSuccess;
 }
 
 }  // namespace
@@ -84,6 +97,7 @@ extern "C" int culamp_lse_rows_sk_noalloc(double *out, const double *x, const do
     if (d < 1) return CULAMP_ERR_INVALID_ARG;
     if (d > MAXD) return CULAMP_ERR_UNSUPPORTED;
     if (!(p > 0.0)) return CULAMP_ERR_INVALID_ARG;
+    if (n > NOALLOC_MAX_ROWS) return CULAMP_ERR_UNSUPPORTED;   // more row blocks than tickets
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return CULAMP_ERR_CUDA;
     NoallocDevice *nd = nullptr;
@@ -131,6 +145,7 @@ extern "C" int culamp_lse_rows_sk_noalloc(double *out, const double *x, const do
     P.colpot = pot;
     P.marg = marg;
     P.out = out;
+    P.use_ref = 1;   // out's incoming value is a hint only: any value gives the same result
     P.finish = FIN_NONE;
     const cudaError_t e = launch_pass(P, pmode_of(p), ACC_LSE, sh, scr, st);
     return e == cudaSuccess ? CULAMP_OK : CULAMP_ERR_CUDA;

@@ -124,7 +124,7 @@ static __global__ void eta_mu_kernel(double *out, const double *c, double alpha_
     if (j < m) out[j] = (c[j] + alpha_over_n) / tau_mu;
 }
 
-// Annealing warm start: ws = v + f (v - prev); prev = v (AnnealedSinkhorn.jl:207-210)
+// Annealing warm start: ws = v + f (v - prev); prev = v (AnnealedSinkhorn.jl:123-126)
 static __global__ void extrapolate_kernel(double *ws, double *prev, const double *v, double f, long long n) {
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i < n) {

@@ -1,5 +1,5 @@
 // solvers.cu -- chosen-form solver drivers: Sinkhorn (SinkhornKernel.jl:477-559),
-// LAMP (MirrorProxKernel.jl:1019-1132) and annealed Sinkhorn (AnnealedSinkhorn.jl:149-261).
+// LAMP (MirrorProxKernel.jl:1019-1132) and annealed Sinkhorn (AnnealedSinkhorn.jl:65-177).
 //
 // A solve is one CUDA graph: a conditional WHILE node whose body holds U
 // unrolled iterations (each a fixed sequence of pair passes) followed by a
@@ -93,6 +93,7 @@ struct culamp_handle_s::Solver {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     struct Cached { GraphKey key; cudaGraphExec_t exec = nullptr; };
     std::vector<Cached> graphs;
+    bool graph_pdl_failed = false;   // conditional bodies did not take programmatic edges
 
     void drop_graphs() {
         for (auto &g : graphs)
@@ -220,16 +221,15 @@ int pick_unroll(double pairs_per_iter) {
     return u;
 }
 
-// Build (or fetch) a WHILE graph whose body runs `body` `unroll` times.
-int get_graph(culamp_handle h, const GraphKey &key, const std::function<cudaError_t(cudaStream_t)> &body,
-              cudaGraphExec_t *out) {
-    Solver &S = *h->solver;
-    for (auto &g : S.graphs)
-        if (g.key == key) { *out = g.exec; return CULAMP_OK; }
+// Build a WHILE graph whose body runs `body` `unroll` times.
+cudaError_t build_while_graph(Solver &S, const GraphKey &key,
+                              const std::function<cudaError_t(cudaStream_t)> &body, cudaGraphExec_t *out) {
+    *out = nullptr;
     cudaGraph_t g = nullptr;
-    CUDA_TRY(h, cudaGraphCreate(&g, 0));
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    if (e != cudaSuccess) return e;
     cudaGraphConditionalHandle ch;
-    cudaError_t e = cudaGraphConditionalHandleCreate(&ch, g, 1, cudaGraphCondAssignDefault);
+    e = cudaGraphConditionalHandleCreate(&ch, g, 1, cudaGraphCondAssignDefault);
     cudaGraphNodeParams np = {};
     cudaGraphNode_t node;
     if (e == cudaSuccess) {
@@ -253,11 +253,39 @@ int get_graph(culamp_handle h, const GraphKey &key, const std::function<cudaErro
             cudaGraph_t captured = nullptr;
             e = cudaStreamEndCapture(S.cap_stream, &captured);
             if (eb != cudaSuccess) e = eb;
+            if (e != cudaSuccess && captured && captured != bodyg) cudaGraphDestroy(captured);
         }
     }
     cudaGraphExec_t exec = nullptr;
     if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, 0);
     cudaGraphDestroy(g);
+    *out = exec;
+    return e;
+}
+
+// Build (or fetch) the WHILE graph of `key`. The passes are recorded with
+// programmatic dependent launches; if the driver cannot keep those edges in a
+// conditional body, the graph is recorded again with plain launches.
+int get_graph(culamp_handle h, const GraphKey &key, const std::function<cudaError_t(cudaStream_t)> &body,
+              cudaGraphExec_t *out, const std::function<void()> &reset = nullptr) {
+    Solver &S = *h->solver;
+    for (auto &g : S.graphs)
+        if (g.key == key) { *out = g.exec; return CULAMP_OK; }
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t e = cudaErrorNotSupported;
+    if (!S.graph_pdl_failed) {
+        if (reset) reset();
+        e = build_while_graph(S, key, body, &exec);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            S.graph_pdl_failed = true;
+        }
+    }
+    if (e != cudaSuccess) {
+        PdlOff plain;
+        if (reset) reset();
+        e = build_while_graph(S, key, body, &exec);
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         return culamp_set_error(h, CULAMP_ERR_CUDA, "graph build: %s", cudaGetErrorString(e));
@@ -516,8 +544,7 @@ int sinkhorn_loop(culamp_handle h, int n, int m, int d, double p, double eta, do
         key.freq = aligned ? frequency : 0;
         key.generation = S.generation;
         cudaGraphExec_t ex = nullptr;
-        body_pos = 0;
-        int s = get_graph(h, key, body, &ex);
+        int s = get_graph(h, key, body, &ex, [&body_pos]() { body_pos = 0; });
         if (s) return s;
         CUDA_TRY(h, cudaGraphLaunch(ex, st));
     }
@@ -1024,7 +1051,7 @@ extern "C" int culamp_annealed_sinkhorn(culamp_handle h, const double *x, const 
     int s = check_solver_args(h, x, y, n, m, d, r, c, args, frequency, p);
     if (s) return s;
     if (!phi || !psi) return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "null output pointer");
-    const double eta_final = args->epsilon;   // AnnealedSinkhorn.jl:162 (Q4)
+    const double eta_final = args->epsilon;   // AnnealedSinkhorn.jl:78 (Q4)
     if (!(eta_final > 0.0))
         return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "annealed Sinkhorn needs epsilon > 0");
     if (!(args->anneal_mult > 0.0 && args->anneal_mult < 1.0) && args->eta_p > eta_final)

@@ -129,6 +129,11 @@ SIGNATURES = {
                                           _U32, C.POINTER(CBatchStats), C.POINTER(CBatchInfo), _VP]),
     "culamp_marginal_error_fp64": (C.c_int, [_VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, _VP, _VP,
                                              _D, _D, _D, C.POINTER(_D), C.POINTER(_D), _VP]),
+    "culamp_sinkhorn_dense": (C.c_int, [_VP, _VP, _I64, _I64, _VP, _VP, C.POINTER(CArgs), _I64, _VP,
+                                        _VP, _VP, _VP, _VP, C.POINTER(CStats), C.POINTER(CLogRow),
+                                        _I64, _VP]),
+    "culamp_lamp_dense": (C.c_int, [_VP, _VP, _I64, _I64, _VP, _VP, C.POINTER(CArgs), _I64, _VP, _VP,
+                                    _VP, _VP, C.POINTER(CStats), C.POINTER(CLogRow), _I64, _VP]),
 }
 
 _lib = None

@@ -7,7 +7,7 @@ solvers so call sites read the same:
 * sinkhorn_euclidean        (SinkhornKernel.jl:579-608)
 * extragradient_color_transfer (MirrorProxKernel.jl:1019-1132)
 * extragradient_euclidean   (MirrorProxKernel.jl:1143-1185)
-* annealed_sinkhorn_euclidean (AnnealedSinkhorn.jl:149-261)
+* annealed_sinkhorn_euclidean (AnnealedSinkhorn.jl:65-177)
 
 Point clouds are (N, d) float64 arrays, point-major -- the memory layout of the
 reference's 3 x N column-major CuArray. CUDA tensors (torch) run the
@@ -93,6 +93,7 @@ class SolveResult:
     nu: object = None
     theta: object = None
     log: list = field(default_factory=list)
+    plan: object = None     # dense solvers: the transport plan (n x m), when requested
 
 
 # ------------------------------------------------------------------ helpers
@@ -344,7 +345,7 @@ def solve_annealed_sinkhorn(x, y, r, c, args: EOTArgs, frequency: int = 10, p: f
 def annealed_sinkhorn_euclidean(marginal1, marginal2, location1, location2, out1: str, out2: str,
                                 potentials: str, args: EOTArgs, frequency: int, p: float,
                                 flags: int = 0):
-    """AnnealedSinkhorn.jl:149-261. Returns (phi, psi, objective)."""
+    """AnnealedSinkhorn.jl:65-177. Returns (phi, psi, objective)."""
     res = solve_annealed_sinkhorn(location1, location2, marginal1, marginal2, args, frequency, p,
                                   flags)
     if args.verbose:

@@ -2,16 +2,18 @@
 #
 # Drop-in for the kernelized path of CuLAMP.jl: the functions below keep the
 # reference's names and signatures (src/solvers/SinkhornKernel.jl:477-489,
-# src/solvers/MirrorProxKernel.jl:1019, src/solvers/AnnealedSinkhorn.jl:149-160)
+# src/solvers/MirrorProxKernel.jl:1019, src/solvers/AnnealedSinkhorn.jl:65-76)
 # and forward device pointers of CuArray{Float64} to the C ABI. A 3 x N
 # column-major CuArray has the point-major layout the library expects.
 #
 # Julia is not installed in the environment this library was built in, so this
 # file has not been executed; it is the binding a maintainer adds next to
-# CuLAMP.jl (see INTEGRATION.md).
+# CuLAMP.jl, whose run_dot / run_ctransfer call sites then dispatch here.
 module CuLAMPB200
 
 using CUDA
+using ChainRulesCore
+using LinearAlgebra: dot
 
 const libculamp = joinpath(@__DIR__, "..", "libculamp_b200.so")
 
@@ -140,7 +142,7 @@ end
     annealed_sinkhorn_euclidean(marginal1, marginal2, location1, location2, out1, out2,
                                 potentials, args, frequency, p)
 
-AnnealedSinkhorn.jl:149-261 on libculamp_b200 (potentials file output kept).
+AnnealedSinkhorn.jl:65-177 on libculamp_b200 (potentials file output kept).
 """
 function annealed_sinkhorn_euclidean(marginal1::CuArray{Float64}, marginal2::CuArray{Float64},
                                      location1::CuArray{Float64}, location2::CuArray{Float64},
@@ -247,6 +249,125 @@ function adjoint_sk(x::CuArray{Float64}, y::CuArray{Float64}, φ::CuArray{Float6
                  Int32, CuPtr{Float64}, CuPtr{Float64}, Float64, Float64, Float64, Ptr{Cvoid}),
                 handle(), g, CU_NULL, x, y, N, M, d, φ, ψ, eps, 1.0, Float64(p), stream_ptr()))
     return g
+end
+
+# ---------------------------------------------------------------- differentiable OT
+
+"""
+    max_cost(x, y, p=2) -> W∞
+
+max_ij C(x_i, y_j) (MirrorProxKernel.jl:280-326 followed by the host maximum),
+exact FP64, one launch (culamp_max_cost without row maxima).
+"""
+function max_cost(x::CuArray{Float64}, y::CuArray{Float64}, p=2)
+    d, N = size(x)
+    M = size(y, 2)
+    w = Ref{Float64}(0.0)
+    check(ccall((:culamp_max_cost, libculamp), Cint,
+                (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Int64, Int64, Int32, Float64,
+                 CuPtr{Float64}, Ref{Float64}, Ptr{Cvoid}),
+                handle(), x, y, N, M, d, Float64(p), CU_NULL, w, stream_ptr()))
+    return w[]
+end
+
+# Solver settings of an entropic-OT value solve: eta_p = eps / W∞, stop at L1 <= tol
+# (the solvers stop at epsilon / 6), the reference defaults elsewhere
+# (src/Utilities.jl:18-31).
+_value_args(eta_p, tol) = CArgs(eta_p, 0.0, 1.0, 1.0, 0.01, 1.0, 6.0 * tol, 0.95, 200_000, 10, Inf,
+                                Int32(0), Int32(0))
+
+"""
+    entropic_ot(x, y, a, b, eps; p=2, tol=1e-7) -> (value, φ, ψ)
+
+OT_eps(a, b; x, y) = min_P <P, C> + eps sum P log P over the couplings of a and b,
+by the kernel Sinkhorn at absolute regularisation eps (eta_p = eps / W∞) to L1
+marginal error tol; value = eps (a.φ + b.ψ), the dual value at the optimum.
+"""
+function entropic_ot(x::CuArray{Float64}, y::CuArray{Float64}, a::CuArray{Float64},
+                     b::CuArray{Float64}, eps::Float64; p=2, tol::Float64=1e-7)
+    d, N = size(x)
+    M = size(y, 2)
+    winf = max_cost(x, y, p)
+    φ = CUDA.zeros(Float64, N)
+    ψ = CUDA.zeros(Float64, M)
+    stats = CStats()
+    cargs = Ref(_value_args(eps / winf, tol))
+    check(ccall((:culamp_sinkhorn, libculamp), Cint,
+                (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Int64, Int64, Int32, CuPtr{Float64},
+                 CuPtr{Float64}, Ptr{CArgs}, Int64, Float64, CuPtr{Float64}, CuPtr{Float64}, UInt32,
+                 CuPtr{Float64}, CuPtr{Float64}, Ref{CStats}, Ptr{CLogRow}, Int64, Ptr{Cvoid}),
+                handle(), x, y, N, M, d, a, b, cargs, 10, Float64(p), CU_NULL, CU_NULL, UInt32(0),
+                φ, ψ, stats, C_NULL, 0, stream_ptr()))
+    return eps * (dot(a, φ) + dot(b, ψ)), φ, ψ
+end
+
+"""
+    entropic_ot_self(x, a, eps; p=2, tol=1e-7) -> (value, f)
+
+OT_eps(a, a; x, x) by the symmetric iteration (one potential f = φ = ψ);
+value = 2 eps a.f.
+"""
+function entropic_ot_self(x::CuArray{Float64}, a::CuArray{Float64}, eps::Float64; p=2,
+                          tol::Float64=1e-7)
+    winf = max_cost(x, x, p)
+    args = _value_args(eps / winf, tol)
+    d, N = size(x)
+    f = CUDA.zeros(Float64, N)
+    stats = CStats()
+    check(ccall((:culamp_symmetric_sinkhorn, libculamp), Cint,
+                (Ptr{Cvoid}, CuPtr{Float64}, Int64, Int32, CuPtr{Float64}, Ptr{CArgs}, Int64, Float64,
+                 CuPtr{Float64}, UInt32, CuPtr{Float64}, Ref{CStats}, Ptr{CLogRow}, Int64, Ptr{Cvoid}),
+                handle(), x, N, d, a, Ref(args), 10, Float64(p), CU_NULL, UInt32(0), f, stats,
+                C_NULL, 0, stream_ptr()))
+    return 2 * eps * dot(a, f), f
+end
+
+"""
+    sinkhorn_divergence(x, y, a, b, eps; p=2, tol=1e-7) -> S
+
+S_eps(a, b; x, y) = OT_eps(a, b) - OT_eps(a, a)/2 - OT_eps(b, b)/2 of the point
+clouds x (d x N) and y (d x M) with weights a, b; eps absolute. Differentiable
+in x, y, a and b through the rrule below.
+"""
+sinkhorn_divergence(x, y, a, b, eps; p=2, tol=1e-7) =
+    first(_divergence_parts(x, y, a, b, eps, p, tol))
+
+function _divergence_parts(x, y, a, b, eps, p, tol)
+    vxy, φ, ψ = entropic_ot(x, y, a, b, Float64(eps); p=p, tol=tol)
+    vxx, f = entropic_ot_self(x, a, Float64(eps); p=p, tol=tol)
+    vyy, g = entropic_ot_self(y, b, Float64(eps); p=p, tol=tol)
+    return vxy - vxx / 2 - vyy / 2, (φ, ψ, f, g)
+end
+
+"""
+    rrule(::typeof(sinkhorn_divergence), x, y, a, b, eps; p=2, tol=1e-7)
+
+Envelope-theorem gradients at the solved potentials, with eps (and so the
+problem) fixed -- W∞ only sets each solve's eta_p = eps / W∞ and does not enter
+the value, so it is treated as a constant:
+  * dS/dx = adjoint(x, y; φ, ψ) - adjoint(x, x; f, f): x enters both sides of
+    OT(a, a), whose plan is symmetric, so its two halves are equal and the
+    factor 1/2 cancels; adjoint(x, y; φ, ψ)_i =
+    sum_j P_ij grad_x C(x_i, y_j) recomputes P_ij = exp(φ_i + ψ_j - C_ij / eps)
+    on the fly (culamp_adjoint_sk) -- nothing N x M is stored;
+  * dS/dy symmetrically; dS/da = eps (φ - f), dS/db = eps (ψ - g) (defined up to a
+    constant, as sum a = sum b = 1).
+eps, p and tol get no tangent.
+"""
+function ChainRulesCore.rrule(::typeof(sinkhorn_divergence), x::CuArray{Float64},
+                              y::CuArray{Float64}, a::CuArray{Float64}, b::CuArray{Float64}, eps;
+                              p=2, tol=1e-7)
+    S, (φ, ψ, f, g) = _divergence_parts(x, y, a, b, eps, p, tol)
+    e = Float64(eps)
+    function sinkhorn_divergence_pullback(ΔS)
+        Δ = unthunk(ΔS)
+        gx = adjoint_sk(x, x, f, f, e, p)
+        dx = @thunk(Δ .* (adjoint_sk(x, y, φ, ψ, e, p) .- gx))
+        gy = adjoint_sk(y, y, g, g, e, p)
+        dy = @thunk(Δ .* (adjoint_sk(y, x, ψ, φ, e, p) .- gy))
+        return (NoTangent(), dx, dy, Δ .* e .* (φ .- f), Δ .* e .* (ψ .- g), NoTangent())
+    end
+    return S, sinkhorn_divergence_pullback
 end
 
 """

@@ -199,7 +199,7 @@ int culamp_lamp(culamp_handle h, const double *x, const double *y, int64_t n, in
                 double *psi, double *theta, culamp_stats *stats, culamp_log_row *log,
                 int64_t log_cap, void *stream);
 
-/* annealed_sinkhorn_euclidean, potentials only (AnnealedSinkhorn.jl:149-261):
+/* annealed_sinkhorn_euclidean, potentials only (AnnealedSinkhorn.jl:65-177):
  * eta_p -> max(anneal_mult * eta, epsilon) stages with extrapolated warm starts;
  * epsilon is both the final eta and the inner tolerance, as in the reference. */
 int culamp_annealed_sinkhorn(culamp_handle h, const double *x, const double *y, int64_t n,
@@ -300,6 +300,38 @@ int culamp_lamp_host(culamp_handle h, const double *x, const double *y, int64_t 
                      double *psi, double *theta, culamp_stats *stats, culamp_log_row *log,
                      int64_t log_cap);
 
+/* ------------------------------------------------------------ dense costs
+ * The GPU solvers of run_dot without --kernel (CmdLineUtils.jl:189-204): a
+ * caller-supplied cost matrix W (n x m, row-major FP64 device memory, e.g. a
+ * --weights CSV divided by max |W| as run_dot does). Every pass streams W or its
+ * transpose (built once per call in the handle's workspace) from HBM.
+ *
+ * sinkhorn_log (Sinkhorn.jl:8-84): psi = log c - LSE_i(-W_ij/eta_p + phi_i),
+ * phi = log r - LSE_j(-W_ij/eta_p + psi_j) per iteration; every `frequency`
+ * iterations an FP64 check of the plan p = exp(-W/eta_p + phi + psi'): log row
+ * (time, iter, feas = |rowsum - r|_1 + |colsum - c|_1, <p, W>, primal, dual), stop
+ * when primal - dual < epsilon/6 and feas < epsilon/6; then the final two
+ * half-steps. phi0 / psi0 may be NULL (zeros). plan (n x m) may be NULL.
+ * Synchronous at check iterations. */
+int culamp_sinkhorn_dense(culamp_handle h, const double *W, int64_t n, int64_t m,
+                          const double *r, const double *c, const culamp_args *args,
+                          int64_t frequency, const double *phi0, const double *psi0,
+                          double *phi, double *psi, double *plan, culamp_stats *stats,
+                          culamp_log_row *log, int64_t log_cap, void *stream);
+
+/* The GPU LAMP on a dense cost (MirrorProx.jl:397-503): W_inf = max |W_ij|,
+ * eta = eta_p / (2 W_inf); per iteration the extragradient step with
+ * infeas(theta, eta_t) = (logZ_i = LSE_j(-(W_ij/(2 W_inf) + theta_j)/eta_t), column mass
+ * res_j = sum_i r_i exp(... - logZ_i)); every `frequency` iterations an FP64 check:
+ * feas = |c - colsum(r .* P)|_1, objective <W, round(r .* P, r, c)> (Utilities.jl:158-165),
+ * primalv / dualv (MirrorProx.jl:7-32); stop when feas < epsilon/2 and
+ * primal - dual < epsilon/2. Outputs theta, nu (m) and optionally the plan
+ * r .* softmax(-(W/(2 W_inf) .+ nu')/eta_t) (n x m, may be NULL). theta0 may be NULL. */
+int culamp_lamp_dense(culamp_handle h, const double *W, int64_t n, int64_t m, const double *r,
+                      const double *c, const culamp_args *args, int64_t frequency,
+                      const double *theta0, double *theta, double *nu, double *plan,
+                      culamp_stats *stats, culamp_log_row *log, int64_t log_cap, void *stream);
+
 /* FP64 re-evaluation of a Sinkhorn-form plan's L1 marginal errors, exp in FP64
  * (used to certify "1e-6 L1, FP64-checked"). Device pointers; synchronous. */
 int culamp_marginal_error_fp64(culamp_handle h, const double *x, const double *y, int64_t n,
@@ -308,17 +340,19 @@ int culamp_marginal_error_fp64(culamp_handle h, const double *x, const double *y
                                double p, double *row_l1, double *col_l1, void *stream);
 
 /* Scratch-free variant of culamp_lse_rows_sk, for callers that cannot let the
- * library allocate device memory when they call it: code recording a CUDA stream
- * capture (cudaMalloc cannot be captured) and hosts that own all device memory
- * through their own pool or budget. No counterpart in the reference (its kernels
- * allocate nothing, but its solvers allocate their caches with CuArray).
+ * library allocate device memory when they call it: hosts that own all device
+ * memory through their own pool or budget and forbid third-party cudaMalloc.
+ * No counterpart in the reference (its kernels allocate nothing, but its
+ * solvers allocate their caches with CuArray).
  * Same arguments and result as culamp_lse_rows_sk, without a handle. Its scratch
  * is fixed file-scope device memory (3 MiB of split partials + 256 KiB of
  * tickets, held on every GPU that loads the library until exit); n is limited
- * to 16,777,216 rows (CULAMP_ERR_UNSUPPORTED beyond). The first call on a device
- * resolves that memory's address and may load the module: make it before any
- * stream capture. All calls share the scratch, so calls that overlap on the GPU
- * race; serialise them. Calls no cudaMalloc / cudaFree. */
+ * to 8,388,608 rows for every d (CULAMP_ERR_UNSUPPORTED beyond, before any
+ * launch). The first call on a device resolves that memory's address and may
+ * load the module: make it before any stream capture; a failed set-up
+ * (CULAMP_ERR_CUDA) is retried by the next call. All calls share the scratch,
+ * so calls that overlap on the GPU race; serialise them. Calls no cudaMalloc /
+ * cudaFree. */
 int culamp_lse_rows_sk_noalloc(double *out, const double *x, const double *y, int64_t n,
                                int64_t m, int32_t d, const double *marg, const double *pot,
                                double reg, double winf, double p, void *stream);

@@ -451,7 +451,7 @@ int or_lamp_kernel(const double *x, const double *y, int64_t n, int64_t m, int d
     return 0;
 }
 
-/* annealed_sinkhorn_euclidean (AnnealedSinkhorn.jl:149-261), potentials only. */
+/* annealed_sinkhorn_euclidean (AnnealedSinkhorn.jl:65-177), potentials only. */
 int or_annealed_sinkhorn_kernel(const double *x, const double *y, int64_t n, int64_t m, int d,
                                 const double *r, const double *c, const or_args *args,
                                 int64_t frequency, double p, int flags, double *phi, double *psi,

@@ -456,3 +456,120 @@ def fp64_marginal_error_sk(x, y, r, c, phi, psi, eta_p, winf, p):
     res_r, _ = sk_residual(x, y, r, phi, psi, eta_p, winf, p)
     res_c, _ = sk_residual(y, x, c, psi, phi, eta_p, winf, p)
     return float(np.abs(res_r).sum()), float(np.abs(res_c).sum())
+
+
+# ------------------------------------------------ dense-cost GPU solvers (numpy)
+
+def np_neg_entropy_rows(P):
+    """neg_entropy(P, dims=2) (Utilities.jl:137-143): sum_j P_ij log P_ij over P > 0."""
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return np.where(P > 0, P * np.log(np.where(P > 0, P, 1.0)), 0.0).sum(1)
+
+
+def np_round(g, mu, nu):
+    """round (Utilities.jl:158-165): rows scaled to <= mu, columns to <= nu, then
+    the rank-one correction of the remaining row / column deficits."""
+    g1 = g * np.minimum(mu / g.sum(1), 1.0)[:, None]
+    g2 = g1 * np.minimum(nu / g1.sum(0), 1.0)[None, :]
+    rmu = mu - g2.sum(1)
+    rnu = nu - g2.sum(0)
+    return g2 + np.outer(rmu, rnu) / np.abs(rmu).sum()
+
+
+def np_primalv(P, W, winf, etap, r, c):
+    """primalv(p, W, W_inf, eta_p, r, c) (MirrorProx.jl:28-32)."""
+    rP = r[:, None] * P
+    return 2 * (0.5 * (W * rP).sum() + (winf * np.abs(rP.sum(0) - c)).sum()
+                + etap * np.dot(r, np_neg_entropy_rows(P)) + etap * np.dot(r, np.log(r)))
+
+
+def np_dualv(theta, W, winf, etap, r, c):
+    """dualv(theta, W, W_inf, eta_p, r, c) (MirrorProx.jl:7-13)."""
+    if etap == 0:
+        return -np.dot(c, 2 * winf * theta) + np.dot(r, (W + 2 * winf * theta[None, :]).min(1))
+    lse = np_lse(-(0.5 * W + winf * theta[None, :]) / etap, 1)
+    return 2 * ((-winf * np.dot(c, theta) - etap * np.dot(r, lse)) + etap * np.dot(r, np.log(r)))
+
+
+def np_theta_res(theta0, res, c, eta_mu_i, eta_mu):
+    """update_theta_residual (MirrorProx.jl:159-180) with W_inf = 1, no clamp:
+    tanh(d/2 + (1 - eta_mu)/2 log((1+theta)/(1-theta))), d = 2 (res - c) / eta_mu_i."""
+    return np.tanh((res - c) / eta_mu_i + 0.5 * (1 - eta_mu) * np.log((1 + theta0) / (1 - theta0)))
+
+
+def np_lamp_dense_gpu(W, r, c, eta_p, itermax, frequency=50, epsilon=1e-4, eta_mu=0.0, tau_p=1.0,
+                      tau_mu=1.0, alpha=0.01, B=1.0):
+    """The GPU LAMP of MirrorProx.jl:397-503 on a dense W (n x m; r: n, c: m).
+    Returns (r .* P, theta, nu, log rows (iter, feas, obj, primal, dual), iterations,
+    eta_t, stopped)."""
+    n, m = W.shape
+    winf = np.abs(W).max()
+    theta = np.zeros(m)
+    etap = eta_p / 2 / winf
+    nu = theta.copy()
+    emu = (c + alpha / m) / tau_mu
+    minv, maxv = math.tanh(-B / 2), math.tanh(B / 2)
+
+    def softmax_rows(th, eta_t):
+        A = np.zeros_like(W) if math.isinf(eta_t) else -(W / (2 * winf) + th[None, :]) / eta_t
+        return np.exp(A - np_lse(A, 1)[:, None])
+
+    def infeas(th, eta_t):
+        return (r[:, None] * softmax_rows(th, eta_t)).sum(0)
+
+    eta_t = math.inf
+    res = infeas(nu, eta_t)
+    log = []
+    stopped, it = 2, 0
+    for it in range(1, itermax + 1):
+        if (it - 1) % frequency == 0:
+            P = softmax_rows(nu, eta_t)
+            rP = r[:, None] * P
+            obj = (W * np_round(rP, r, c)).sum()
+            primal = np_primalv(P, W, winf, etap, r, c)
+            dual = np_dualv(theta, W, winf, etap, r, c)
+            feas = np.abs(c - rP.sum(0)).sum()
+            log.append((it, feas, obj, primal, dual))
+            if feas < epsilon / 2 and primal - dual < epsilon / 2:
+                stopped = 1
+                break
+        thb = np_theta_res(theta, res, c, emu, tau_mu * eta_mu)
+        eta_t = 1 / (tau_p + (1 / eta_t) * (1 - etap))
+        nub = tau_p * eta_t * theta + (1 - tau_p * eta_t) * nu
+        res = infeas(nub, eta_t)
+        theta = np_theta_res(theta, res, c, emu, eta_mu)
+        nu = (1 - tau_p * eta_t) * nu + tau_p * eta_t * thb
+        theta = np.clip(theta, minv, maxv)
+        res = infeas(nu, eta_t)
+    plan = r[:, None] * softmax_rows(nu, eta_t)
+    return plan, theta, nu, log, it, eta_t, stopped
+
+
+def np_sinkhorn_dense(W, r, c, eta_p, itermax, frequency=50, epsilon=1e-4):
+    """sinkhorn_log (Sinkhorn.jl:8-84) for any n x m W. Returns (p, phi, psi, log
+    rows (iter, feas, obj, pobj, dobj), iterations, num_iter, stopped)."""
+    n, m = W.shape
+    K = -W / eta_p
+    phi, psi = np.zeros(n), np.zeros(m)
+    log, num_iter, stopped, it = [], 0, 2, 0
+    for it in range(1, itermax + 1):
+        psi = np.log(c) - np_lse(K + phi[:, None], 0)
+        phi = np.log(r) - np_lse(K + psi[None, :], 1)
+        if (it - 1) % frequency == 0:
+            p = np.exp(K + phi[:, None] + psi[None, :])
+            feas = np.abs(p.sum(0) - c).sum() + np.abs(p.sum(1) - r).sum()
+            obj = (p * W).sum()
+            with np.errstate(divide="ignore", invalid="ignore"):
+                ent = np.where(p > 0, p * np.log(np.where(p > 0, p, 1.0)), 0.0).sum()
+            pobj = obj + eta_p * ent
+            X = K + phi[:, None] + psi[None, :]
+            lse_all = np.log(np.exp(X - X.max()).sum()) + X.max()
+            dobj = -eta_p * (-lse_all - np.dot(c, psi) - np.dot(r, phi))
+            log.append((it, feas, obj, pobj, dobj))
+            if pobj - dobj < epsilon / 6 and feas < epsilon / 6:
+                stopped = 1
+                break
+        num_iter += 1
+    psi = np.log(c) - np_lse(K + phi[:, None], 0)
+    phi = np.log(r) - np_lse(K + psi[None, :], 1)
+    return np.exp(K + phi[:, None] + psi[None, :]), phi, psi, log, it, num_iter, stopped
