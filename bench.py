@@ -558,6 +558,7 @@ def extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_chosen, chosen_ms):
         "chosen_over_plain_per_iter": (pl5.elapsed_ms / max(1, pl5.iterations)) /
                                       (l5.elapsed_ms / max(1, l5.iterations))}
     ex["features_16384_d256"] = feature_extra(cb, D, torch, dev)
+    ex["dense_grid4096"] = dense_extra(cb, D, torch, np, dev)
     ex["divergence_65536"] = divergence_extra(cb, D, torch, dev, X5, Y5, R5, C5, s5.winf)
     return ex
 
@@ -663,6 +664,39 @@ def batched_extra(cb, D, torch, np, dev, dfma, ex2, count=512, sample=24):
             "weighted_roofline_frac": ideal_s / (out.elapsed_ms * 1e-3),
             "sequential_ms_estimate": seq_ms * tot_pairs / max(seq_pairs, 1.0),
             "sequential_sample": sample}
+
+
+def dense_extra(cb, D, torch, np, dev):
+    """Dense-cost GPU solvers (run_dot without --kernel): the 64x64 grid's
+    squared-Euclidean cost as a 4096 x 4096 FP64 matrix W / max W (134 MB in
+    HBM), eta_p = 1e-3. sinkhorn_log: 200 iterations (two passes over W or W^T
+    each, a check every 50); the pass is HBM-bound (8 bytes per element), so its
+    roofline is the measured HBM bandwidth. LAMP (MirrorProx.jl:397-503):
+    100 iterations (four passes each, a check every 50)."""
+    from culamp_b200.dense import solve_lamp_dense, solve_sinkhorn_dense
+    x, y, r, c = instance()
+    W = D.dense_grid_cost(GRID, GRID)
+    W = torch.as_tensor(W / np.abs(W).max(), device=dev)
+    R, Cc = torch.as_tensor(r, device=dev), torch.as_tensor(c, device=dev)
+    n = W.shape[0]
+    peaks = load_peaks() or {}
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    out = {"n": n, "m": n, "bytes_per_pass": 8.0 * n * n, "peak_hbm_gbs": hbm,
+           "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback"}
+    a = cb.EOTArgs(eta_p=1e-3, epsilon=0.0, itermax=10, verbose=False)
+    solve_sinkhorn_dense(W, R, Cc, a, 50)
+    res = solve_sinkhorn_dense(W, R, Cc, a.copy(itermax=200), 50)
+    # per iteration: 2 passes; 4 check passes every 50 iterations (+1 transpose, +1 final check)
+    passes = 2 * res.iterations + 2 * (res.iterations // 50 + 2) + 1
+    gbs = passes * 8.0 * n * n / (res.elapsed_ms * 1e-3) / 1e9
+    out["sinkhorn"] = {"iterations": res.iterations, "ms": res.elapsed_ms,
+                       "ms_per_iter": res.elapsed_ms / res.iterations, "achieved_gbs": gbs,
+                       "frac_hbm": gbs / hbm, "residual": res.residual}
+    b = cb.EOTArgs(eta_p=1e-3, epsilon=0.0, itermax=100, verbose=False)
+    lr = solve_lamp_dense(W, R, Cc, b, 50, want_plan=False)
+    out["lamp"] = {"iterations": lr.iterations, "ms": lr.elapsed_ms,
+                   "ms_per_iter": lr.elapsed_ms / lr.iterations, "residual": lr.residual}
+    return out
 
 
 def feature_extra(cb, D, torch, dev, n=16384, d=256):

@@ -17,6 +17,16 @@ One iteration, identical in arithmetic to the single-GPU solver:
     transport cost are summed over shards (all_reduce SUM) and every rank takes
     the same stopping decision.
 
+Row-sharded LAMP (sharded_lamp, MirrorProxKernel.jl:1019-1132) splits the
+rows the same way; its column quantities are sums over all rows, so each
+shard computes partial column masses (and costs on check iterations) over its
+rows (culamp_col_residual_spp) and one all_reduce(SUM) of the m-vector per
+infeas(.) call gives the full residual; theta, nu, theta_bar, nu_bar and the
+eta_t / s recursions are replicated and bit-identical on every rank (they
+only see all-reduced values). The row-weighted scalars of the primal / dual
+values (r.logZ, r.LSE(theta) or r.min) are shard sums, all-reduced on check
+iterations.
+
 A process may own several shards (its row blocks are reduced locally first),
 so the same driver runs one rank per GPU over NCCL, several row blocks on one
 GPU, or -- with compute ops that run on the host -- gloo ranks on CPU. Every
@@ -65,6 +75,18 @@ class CudaOps:
     def residual(self, x, y, marg, phi, psi, reg, winf, p):
         res, cost = K.residual_opt(x, y, marg, phi, psi, reg, winf, p)
         return res.abs().sum(), cost.sum()
+
+    def spp_lse(self, out, x, y, theta, reg, st, winf, p):
+        K.warp_logsumexp_spp_ct_fused(x, y, theta, reg, st, winf, p, out=out)
+
+    def col_residual(self, x, y, r, theta, logz, reg, st, winf, p):
+        return K.residual_spp_c(x, y, r, theta, logz, reg, st, winf, p)
+
+    def min_reduce(self, x, y, theta, winf, p):
+        return K.warp_min_reduce(x, y, theta, winf, p)
+
+    def theta_update(self, theta0, res, c, emu, eta_mu, adjust, minv, maxv):
+        return K.update_theta_residual(theta0, res, c, emu, eta_mu, adjust, minv, maxv, 1.0)
 
     def combine(self, parts):
         g, m = parts.shape
@@ -149,3 +171,114 @@ def sharded_sinkhorn(x_shards, r_shards, y, c, args: EOTArgs, frequency: int = 1
     s = resid()
     return ShardedResult(phis, psi, float(s[0]), float(s[1]), it, num_iter, winf, stopped,
                          time.perf_counter() - t0)
+
+
+@dataclass
+class ShardedLampResult:
+    nu: torch.Tensor     # averaged dual (replicated)
+    theta: torch.Tensor  # (replicated)
+    phi: list            # this rank's log r - logZ, one tensor per shard
+    psi: torch.Tensor    # -2 W_inf nu / eta_p (replicated)
+    residual: float
+    objective: float
+    iterations: int
+    winf: float
+    eta_t: float
+    s_t: float
+    stopped: int         # 1 tolerance, 2 itermax, 3 tmax
+    log: list            # (iter, infeas, ot_objective, primal, dual) per check
+    elapsed_s: float
+
+
+def sharded_lamp(x_shards, r_shards, y, c, args: EOTArgs, frequency: int = 100, p: float = 2.0,
+                 check: bool | None = None, marginal_only: bool = False, group=None,
+                 ops=None) -> ShardedLampResult:
+    """Kernel LAMP (MirrorProxKernel.jl:1019-1132) with the rows split over
+    shards and ranks (see module doc). `check` defaults to args.verbose (the
+    reference checks only when verbose, :1081); marginal_only drops the gap
+    test of :1098. Every rank takes the same collective steps."""
+    ops = ops or CudaOps()
+    if frequency < 1:
+        raise ValueError("frequency must be >= 1")
+    if len(x_shards) != len(r_shards) or not x_shards:
+        raise ValueError("one row marginal per x shard")
+    dev = y.device
+    m = y.shape[0]
+    check = bool(args.verbose) if check is None else bool(check)
+    winf_t = torch.tensor([max(ops.max_cost(x, y, p) for x in x_shards)], dtype=torch.float64, device=dev)
+    winf = float(_reduce(winf_t, dist.ReduceOp.MAX, group).item())
+    n_t = torch.tensor([float(sum(x.shape[0] for x in x_shards))], dtype=torch.float64, device=dev)
+    n_total = float(_reduce(n_t, dist.ReduceOp.SUM, group).item())
+    hr_t = torch.zeros(1, dtype=torch.float64, device=dev)
+    for r in r_shards:
+        hr_t += (r * torch.log(r)).sum()
+    eta = args.eta_p / (2.0 * winf)
+    hr = eta * float(_reduce(hr_t, dist.ReduceOp.SUM, group).item())
+    emu = (c + args.alpha / n_total) / args.tau_mu
+    theta = torch.zeros(m, dtype=torch.float64, device=dev)
+    nu = torch.zeros(m, dtype=torch.float64, device=dev)
+    s_t, eta_t, tau_p = 1.0, math.inf, 1.0       # tau_p hard-coded in the reference (:1073)
+    minv, maxv = math.tanh(-args.B / 2.0), math.tanh(args.B / 2.0)
+    logz = [torch.zeros(x.shape[0], dtype=torch.float64, device=dev) for x in x_shards]
+
+    def infeas(th, et, st, want_cost=False):
+        """Column mass (and cost) over all rows; row logZ of the shards."""
+        acc = torch.zeros(2 * m, dtype=torch.float64, device=dev)
+        for x, r, lz in zip(x_shards, r_shards, logz):
+            ops.spp_lse(lz, x, y, th, et, st, winf, p)
+            res, cost = ops.col_residual(x, y, r, th, lz, et, st, winf, p)
+            acc[:m] += res
+            if want_cost:
+                acc[m:] += cost
+        _reduce(acc, dist.ReduceOp.SUM, group)
+        return acc[:m], acc[m:]
+
+    def shard_dot(vals):
+        t = torch.zeros(1, dtype=torch.float64, device=dev)
+        for r, v in zip(r_shards, vals):
+            t += torch.dot(r, v)
+        return float(_reduce(t, dist.ReduceOp.SUM, group).item())
+
+    t0 = time.perf_counter()
+    log, stopped, it = [], 2, 0
+    for it in range(1, args.itermax + 1):
+        el = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
+        if float(_reduce(el, dist.ReduceOp.MAX, group).item()) > args.tmax:
+            stopped = 3
+            it -= 1
+            break
+        if check and (it - 1) % frequency == 0:
+            res, cost = infeas(nu, eta_t, s_t, want_cost=True)
+            residual_value = float((res - c).abs().sum())
+            objective = float(cost.sum())
+            q = eta / eta_t
+            primal = (objective * (1.0 - q) - q * float(torch.dot(res, nu)) + q * shard_dot(logz)
+                      + 2.0 * winf * residual_value)
+            if eta > 0:
+                tmp = []
+                for x in x_shards:
+                    t = torch.empty(x.shape[0], dtype=torch.float64, device=dev)
+                    ops.spp_lse(t, x, y, theta, eta, 1.0, winf, p)
+                    tmp.append(t)
+                dual = -2.0 * eta * shard_dot(tmp) - 2.0 * winf * float(torch.dot(c, theta)) + 2.0 * hr
+            else:
+                tmp = [ops.min_reduce(x, y, theta, winf, p) for x in x_shards]
+                dual = shard_dot(tmp) - 2.0 * winf * float(torch.dot(c, theta))
+            log.append((it, residual_value, objective, primal, dual))
+            gap_ok = True if marginal_only else (primal - dual < args.epsilon / 6.0)
+            if gap_ok and residual_value < args.epsilon / 6.0:
+                stopped = 1
+                break
+        res, _ = infeas(nu, eta_t, s_t)
+        thb = ops.theta_update(theta, res, c, emu, args.eta_mu, False, minv, maxv)
+        eta_t = 1.0 / (tau_p + (1.0 / eta_t) * (1.0 - eta))
+        nub = (1.0 - eta_t) * nu + eta_t * theta
+        s_t = (1.0 - eta_t) * s_t + eta_t
+        res, _ = infeas(nub, eta_t, s_t)
+        theta = ops.theta_update(theta, res, c, emu, args.eta_mu, True, minv, maxv)
+        nu = (1.0 - eta_t) * nu + eta_t * thb
+    res, cost = infeas(nu, eta_t, s_t, want_cost=True)
+    phis = [torch.log(r) - lz for r, lz in zip(r_shards, logz)]
+    psi = -2.0 * winf * nu / args.eta_p if args.eta_p != 0 else torch.full_like(nu, math.nan)
+    return ShardedLampResult(nu, theta, phis, psi, float((res - c).abs().sum()), float(cost.sum()), it, winf,
+                             eta_t, s_t, stopped, log, time.perf_counter() - t0)

@@ -573,3 +573,42 @@ def np_sinkhorn_dense(W, r, c, eta_p, itermax, frequency=50, epsilon=1e-4):
     psi = np.log(c) - np_lse(K + phi[:, None], 0)
     phi = np.log(r) - np_lse(K + psi[None, :], 1)
     return np.exp(K + phi[:, None] + psi[None, :]), phi, psi, log, it, num_iter, stopped
+
+
+# ------------------------------------------------ cell-similarity feature costs
+
+def np_cell_cost(data, metric, normalize_features=True):
+    """feature_cost(kernel, i, j) of CellUtilities.jl:127-172 for all row pairs
+    of one data matrix (rows = points), with CellCostKernel's statistics
+    (:69-112): row sums s_i (0 -> 1, or all 1 when not normalising), squared
+    norms, means and centred squared norms of the raw rows, metric scale
+    l1: 2, l2: sqrt(2), cosine / correlation: 2."""
+    a = np.asarray(data, dtype=np.float64)
+    n, d = a.shape
+    s = a.sum(1) if normalize_features else np.ones(n)
+    if normalize_features:
+        s = np.where(s > 0, s, 1.0)
+    sq = (a * a).sum(1)
+    mean = a.mean(1)
+    csq = ((a - mean[:, None]) ** 2).sum(1)
+    metric = "correlation" if metric == "pearson" else metric
+    scale = {"l1": 2.0, "l2": math.sqrt(2.0), "cosine": 2.0, "correlation": 2.0}[metric]
+    if metric == "l1":
+        u = a / s[:, None]
+        return np.abs(u[:, None, :] - u[None, :, :]).sum(-1) / scale
+    dot = (a @ a.T) / (s[:, None] * s[None, :])
+    nrm = sq / s ** 2
+    if metric == "l2":
+        return np.sqrt(np.maximum(nrm[:, None] + nrm[None, :] - 2 * dot, 0.0)) / scale
+    if metric == "cosine":
+        den = np.sqrt(nrm[:, None] * nrm[None, :])
+        with np.errstate(divide="ignore", invalid="ignore"):
+            sim = np.clip(dot / den, -1.0, 1.0)
+        return np.where(den > 0, (1.0 - sim) / scale, 0.0)
+    mu = mean / s
+    cen = csq / s ** 2
+    den = np.sqrt(cen[:, None] * cen[None, :])
+    with np.errstate(divide="ignore", invalid="ignore"):
+        corr = np.clip((dot - d * mu[:, None] * mu[None, :]) / den, -1.0, 1.0)
+    special = np.where(np.abs(mu[:, None] - mu[None, :]) <= math.sqrt(np.finfo(float).eps), 0.0, 1.0 / scale)
+    return np.where(den > 0, (1.0 - corr) / scale, special)

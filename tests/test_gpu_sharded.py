@@ -85,6 +85,38 @@ def test_row_blocks_stop_at_the_oracle_iteration(oracle, p, frequency, shards):
     assert res.num_iter == one.num_iter == wst.num_iter
 
 
+@pytest.mark.parametrize("p,eta_p", [(2.0, 1e-2), (1.0, 1e-2), (2.0, 0.0)])
+@pytest.mark.parametrize("shards", [2, 3])
+def test_row_blocks_lamp_match_single_solver_and_oracle(oracle, p, eta_p, shards):
+    """Row-sharded LAMP through the real passes (partial column masses summed
+    over the blocks): nu / theta against the single-GPU LAMP and the oracle,
+    the log rows (marginal, objective, primal, dual) and eta_t exactly."""
+    import torch
+    import culamp_b200 as cb
+    from culamp_b200 import datasets as D
+    from culamp_b200.sharded import shard_rows, sharded_lamp
+    x, y, r, c = D.grid_instance(20, 20, "mixture")
+    X, Y, R, Cc = (torch.as_tensor(v, device="cuda") for v in (x, y, r, c))
+    blocks = [shard_rows(x.shape[0], shards, k) for k in range(shards)]
+    a = cb.EOTArgs(eta_p=eta_p, epsilon=1e-12, itermax=80, verbose=True, B=1.1)
+    res = sharded_lamp([X[s:e].contiguous() for s, e in blocks], [R[s:e].contiguous() for s, e in blocks],
+                       Y, Cc, a, frequency=10, p=p)
+    one = cb.solve_lamp(X, Y, R, Cc, a, 10, p)
+    nu, _, _, theta, wst, log = oracle.lamp_kernel(x, y, r, c, oracle.Args(eta_p=eta_p, epsilon=1e-12, itermax=80,
+                                                                           verbose=True, B=1.1), frequency=10, p=p)
+    assert res.iterations == one.iterations == wst.iterations
+    assert res.eta_t == one.eta_t == wst.eta_t
+    got_nu = res.nu.cpu().numpy()
+    np.testing.assert_allclose(gauge(got_nu, c), gauge(one.nu.cpu().numpy(), c), atol=2e-6, rtol=0)
+    np.testing.assert_allclose(gauge(got_nu, c), gauge(nu, c), atol=2e-6, rtol=0)
+    np.testing.assert_allclose(res.theta.cpu().numpy(), theta, atol=5e-6, rtol=0)
+    got = np.array(res.log)
+    want = np.array([row[1:6] for row in log])
+    assert got.shape == want.shape and np.array_equal(got[:, 0], want[:, 0])
+    np.testing.assert_allclose(got[:, 1], want[:, 1], rtol=1e-3, atol=1e-9)
+    np.testing.assert_allclose(got[:, 2:], want[:, 2:], rtol=1e-4, atol=1e-6)
+
+
 def test_single_rank_nccl_group(tmp_path):
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     script = f"""

@@ -31,6 +31,21 @@ class OracleOps:
         res, cost = self.O.sk_residual(x.numpy(), y.numpy(), marg.numpy(), phi.numpy(), psi.numpy(), reg, winf, p)
         return float(np.abs(res).sum()), float(np.sum(cost))
 
+    def spp_lse(self, out, x, y, theta, reg, st, winf, p):
+        out.copy_(torch.from_numpy(self.O.spp_lse(x.numpy(), y.numpy(), theta.numpy(), reg, st, winf, p)))
+
+    def col_residual(self, x, y, r, theta, logz, reg, st, winf, p):
+        res, cost = self.O.spp_col_residual(x.numpy(), y.numpy(), r.numpy(), theta.numpy(), logz.numpy(),
+                                            reg, st, winf, p)
+        return torch.from_numpy(res), torch.from_numpy(cost)
+
+    def min_reduce(self, x, y, theta, winf, p):
+        return torch.from_numpy(self.O.min_reduce(x.numpy(), y.numpy(), theta.numpy(), winf, p))
+
+    def theta_update(self, theta0, res, c, emu, eta_mu, adjust, minv, maxv):
+        return torch.from_numpy(self.O.theta_update(theta0.numpy(), res.numpy(), c.numpy(), emu.numpy(),
+                                                    eta_mu, adjust, minv, maxv, 1.0))
+
     def combine(self, parts):
         a = -parts.numpy()
         mx = a.max(0)
@@ -62,6 +77,18 @@ def _worker(rank, world, port, case, out_dir, oracle_dir):
     blocks = [shard_rows(x.shape[0], world * per_rank, rank * per_rank + k) for k in range(per_rank)]
     xs = [x[a:b].contiguous() for a, b in blocks]
     rs = [r[a:b].contiguous() for a, b in blocks]
+    if case.get("lamp"):
+        from culamp_b200.sharded import sharded_lamp
+        a = EOTArgs(eta_p=case["eta_p"], epsilon=case["epsilon"], itermax=case["itermax"], verbose=True,
+                    B=case["B"])
+        res = sharded_lamp(xs, rs, y, c, a, frequency=case["frequency"], p=case["p"], ops=OracleOps(O),
+                           marginal_only=case["marginal_only"])
+        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), phi=np.concatenate([v.numpy() for v in res.phi]),
+                 psi=res.psi.numpy(), nu=res.nu.numpy(), theta=res.theta.numpy(), log=np.array(res.log),
+                 stats=np.array([res.iterations, res.stopped, res.residual, res.objective, res.winf,
+                                 res.eta_t, res.s_t]))
+        dist.destroy_process_group()
+        return
     a = EOTArgs(eta_p=case["eta_p"], epsilon=case["epsilon"], itermax=case["itermax"], verbose=False)
     res = sharded_sinkhorn(xs, rs, y, c, a, frequency=case["frequency"], p=case["p"], ops=OracleOps(O))
     np.savez(os.path.join(out_dir, f"rank{rank}.npz"), phi=np.concatenate([v.numpy() for v in res.phi]),
@@ -116,3 +143,34 @@ def test_shard_rows_cover_every_row_once():
             assert blocks[0][0] == 0 and blocks[-1][1] == n
             assert all(b[0] == a[1] for a, b in zip(blocks, blocks[1:]))
             assert max(b - a for a, b in blocks) - min(b - a for a, b in blocks) <= 1
+
+
+@pytest.mark.parametrize("p,eta_p,shards_per_rank,marginal_only", [(2.0, 5e-2, 1, False), (1.0, 5e-2, 2, True),
+                                                                   (math.inf, 0.0, 1, False)])
+def test_two_gloo_ranks_lamp_match_single_oracle(oracle, tmp_path, p, eta_p, shards_per_rank, marginal_only):
+    """Row-sharded LAMP: partial column masses all-reduced per infeas(.) call;
+    the replicated duals, eta_t / s recursion, log rows and the gathered row
+    potentials equal the single-process oracle to FP64 rounding."""
+    x, r = _grid(6, 2)
+    y, c = _grid(7, 3)
+    x = x[:-5]
+    r = r[:-5] / r[:-5].sum()
+    case = {"data": (x, y, r, c), "eta_p": eta_p, "epsilon": 1e-12, "itermax": 60, "frequency": 7, "p": p,
+            "shards_per_rank": shards_per_rank, "lamp": True, "B": 1.1, "marginal_only": marginal_only}
+    phi, _, st, outs = _run(case, tmp_path)
+    for o in outs[1:]:
+        assert np.array_equal(o["nu"], outs[0]["nu"]) and np.array_equal(o["stats"], outs[0]["stats"])
+    flags = oracle.CHECK_ALWAYS | (oracle.MARGINAL_ONLY if marginal_only else 0)
+    args = oracle.Args(eta_p=eta_p, epsilon=1e-12, itermax=60, verbose=True, B=1.1)
+    nu, wphi, psi, theta, wst, log = oracle.lamp_kernel(x, y, r, c, args, frequency=7, p=p, flags=flags)
+    o = outs[0]
+    assert int(o["stats"][0]) == wst.iterations
+    assert o["stats"][5] == wst.eta_t and o["stats"][6] == wst.s_t
+    np.testing.assert_allclose(o["nu"], nu, rtol=0, atol=ATOL)
+    np.testing.assert_allclose(o["theta"], theta, rtol=0, atol=ATOL)
+    np.testing.assert_allclose(phi, wphi, rtol=0, atol=1e-9)
+    want = np.array([row[1:6] for row in log])
+    assert o["log"].shape == want.shape and np.array_equal(o["log"][:, 0], want[:, 0])
+    np.testing.assert_allclose(o["log"][:, 1:], want[:, 1:], rtol=1e-10, atol=1e-12)
+    assert o["stats"][2] == pytest.approx(wst.residual, rel=1e-8, abs=1e-14)
+    assert o["stats"][3] == pytest.approx(wst.objective, rel=1e-12)
