@@ -590,7 +590,9 @@ static __device__ __noinline__ void run_finish(const PassParams &P, const double
     }
 }
 
-// Block-wide FP64 sum of up to 4 values per thread; result valid in thread 0.
+// Block-wide FP64 sum of up to 4 values per thread (NT threads); result valid
+// in thread 0. red holds 4 * NT / 32 doubles.
+template <int NT = TPB>
 __device__ __forceinline__ void block_sum4(double (&v)[4], double *red) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -607,14 +609,15 @@ __device__ __forceinline__ void block_sum4(double (&v)[4], double *red) {
     if (threadIdx.x == 0) {
         for (int k = 0; k < 4; ++k) {
             double s = 0.0;
-            for (int ww = 0; ww < TPB / 32; ++ww) s += red[ww * 4 + k];
+            for (int ww = 0; ww < NT / 32; ++ww) s += red[ww * 4 + k];
             v[k] = s;
         }
     }
 }
 
 
-// Block-wide FP64 max of one value; result valid in thread 0.
+// Block-wide FP64 max of one value (NT threads); result valid in thread 0.
+template <int NT = TPB>
 __device__ __forceinline__ double block_max1(double x, double *red) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_down_sync(0xffffffffu, x, o));
@@ -623,7 +626,7 @@ __device__ __forceinline__ double block_max1(double x, double *red) {
     if (l == 0) red[w] = x;
     __syncthreads();
     if (threadIdx.x == 0)
-        for (int ww = 1; ww < TPB / 32; ++ww) x = fmax(x, red[ww]);
+        for (int ww = 1; ww < NT / 32; ++ww) x = fmax(x, red[ww]);
     return x;
 }
 
@@ -825,15 +828,25 @@ __device__ __forceinline__ void fr_col2(const double4 c0, const double4 c1, cons
     }
 }
 
+// Synchronises the threads that stage one column tile together: the CTA
+// (GT = TPB) or one warp (GT = 32, the wide small-problem pass).
+template <int GT>
+__device__ __forceinline__ void group_sync() {
+    if constexpr (GT == 32) __syncwarp();
+    else __syncthreads();
+}
+
 // Returns false when a real row's partial sum overflowed the window (a term
-// clamped high, or a non-finite input).
-template <int PM, int D, int R>
+// clamped high, or a non-finite input). GT threads (the CTA, or one warp)
+// share the staged column tile; thread g of the group owns rows
+// row_base + g + r * GT.
+template <int PM, int D, int R, int GT = TPB>
 __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double alpha, double beta,
                                                   int row_base, int cbeg, int cend, double *smem,
                                                   double (&Mo)[R], double (&So)[R],
                                                   double (&Ho)[R]) {
     constexpr bool SQ = (PM == P_SQ);
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x % GT;
     const double a2 = alpha * LOG2E;
     const double cb = P.colpot_unit ? LOG2E : beta * LOG2E;
     double ctr[D];
@@ -845,7 +858,7 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
     acc.zero();
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        const int row = row_base + tid + r * TPB;
+        const int row = row_base + tid + r * GT;
         const bool ok = row < P.n;
         double h = 0.0;
 #pragma unroll
@@ -860,8 +873,8 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
     }
     double4 *tile = reinterpret_cast<double4 *>(smem);
     for (int c0 = cbeg; c0 < cend; c0 += CHUNK) {
-        __syncthreads();
-        for (int q = tid; q < CHUNK; q += TPB) {
+        group_sync<GT>();
+        for (int q = tid; q < CHUNK; q += GT) {
             const int j = c0 + q;
             double4 v = make_double4(0.0, 0.0, 0.0, -INFINITY);
             if (j < cend) {
@@ -879,7 +892,7 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
             }
             tile[q] = v;
         }
-        __syncthreads();
+        group_sync<GT>();
         const int nc = min(CHUNK, cend - c0);
         int q = 0;
         // few rows per thread (small problems): unroll more columns so each warp
@@ -903,7 +916,7 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
     bool good = true;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        const int row = row_base + tid + r * TPB;
+        const int row = row_base + tid + r * GT;
         const bool real_row = row < P.n;
         double h = 0.0;
 #pragma unroll
@@ -923,14 +936,15 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
 }
 
 // Packed (d <= 3) log-sum-exp tile: rows in registers, column tiles of CHUNK
-// (y - ctr, g) double4 entries in shared memory, broadcast to the warp.
-template <int PM, int D, int R, bool MOM, int UNROLL = 8>
+// (y - ctr, g) double4 entries in shared memory, broadcast to the warp. GT
+// threads share the staged tile, as in tile_lse_fixedref.
+template <int PM, int D, int R, bool MOM, int UNROLL = 8, int GT = TPB>
 __device__ __forceinline__ void tile_lse_packed(const PassParams &P, double alpha, double beta,
                                                 int row_base, int cbeg, int cend, double *smem,
                                                 double (&Mo)[R], double (&So)[R],
                                                 double (&MOMo)[R], double (&Ho)[R]) {
     constexpr bool SQ = (PM == P_SQ);
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x % GT;
     const double a2 = alpha * LOG2E;
     const double cb = P.colpot_unit ? LOG2E : beta * LOG2E;
     double ctr[D];
@@ -942,7 +956,7 @@ __device__ __forceinline__ void tile_lse_packed(const PassParams &P, double alph
     float S[R], Cc[R], cs[R], mo[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        const int row = row_base + tid + r * TPB;
+        const int row = row_base + tid + r * GT;
         const bool ok = row < P.n;
         double h = 0.0;
 #pragma unroll
@@ -958,8 +972,8 @@ __device__ __forceinline__ void tile_lse_packed(const PassParams &P, double alph
     }
     double4 *tile = reinterpret_cast<double4 *>(smem);
     for (int c0 = cbeg; c0 < cend; c0 += CHUNK) {
-        __syncthreads();
-        for (int q = tid; q < CHUNK; q += TPB) {
+        group_sync<GT>();
+        for (int q = tid; q < CHUNK; q += GT) {
             const int j = c0 + q;
             double4 v = make_double4(0.0, 0.0, 0.0, -INFINITY);
             if (j < cend) {
@@ -977,7 +991,7 @@ __device__ __forceinline__ void tile_lse_packed(const PassParams &P, double alph
             }
             tile[q] = v;
         }
-        __syncthreads();
+        group_sync<GT>();
         const int nc = min(CHUNK, cend - c0);
         int q = 0;
         for (; q + 8 <= nc; q += 8) {
@@ -999,12 +1013,13 @@ __device__ __forceinline__ void tile_lse_packed(const PassParams &P, double alph
 }
 
 // Per-row epilogue of a reduction pass (one thread per output row, R rows per
-// thread) and the grid-level finish step run by the last CTA of the grid.
-template <int ACC, int R>
+// thread, NT threads of which the first `rows_blk` / R own rows) and the
+// grid-level finish step run by the last CTA of the grid.
+template <int ACC, int R, int NT = TPB>
 __device__ __forceinline__ void row_epilogue(const PassParams &P, int rb, int row_base, double beta,
                                              const double (&Mv)[R], const double (&Sv)[R],
                                              const double (&MOMv)[R], const double (&Hv)[R],
-                                             double *red, int &s_last, int nrb) {
+                                             double *red, int &s_last, int nrb, int rows_blk = NT * R) {
     Ctl *ctl = P.ctl;
     double acc4[4] = {0.0, 0.0, 0.0, 0.0};
     double amax = -INFINITY;
@@ -1013,8 +1028,9 @@ __device__ __forceinline__ void row_epilogue(const PassParams &P, int rb, int ro
     else if (P.lamp_step == LAMP_B) en = ctl->eta_next;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        const int o = row_base + threadIdx.x + r * TPB;
-        if (o >= P.n) continue;
+        const int lo = threadIdx.x + r * NT;
+        const int o = row_base + lo;
+        if (o >= P.n || lo >= rows_blk) continue;
         if (ACC != ACC_LSE) {
             if (P.out) P.out[o] = Mv[r];
             amax = fmax(amax, Mv[r]);
@@ -1092,10 +1108,10 @@ __device__ __forceinline__ void row_epilogue(const PassParams &P, int rb, int ro
 
     if (P.finish == FIN_NONE) return;
     if (ACC == ACC_MAX) {
-        const double bm = block_max1(amax, red);
+        const double bm = block_max1<NT>(amax, red);
         acc4[0] = bm;
     } else {
-        block_sum4(acc4, red);
+        block_sum4<NT>(acc4, red);
     }
     if (threadIdx.x == 0) {
         for (int k = 0; k < 4; ++k) P.blk[rb * 4 + k] = acc4[k];
@@ -1292,6 +1308,127 @@ __global__ void __launch_bounds__(TPB, (R > RPT_MID) ? 3 : 4)
 #undef CULAMP_RB
 #undef CULAMP_SP
 #undef CULAMP_NRB
+}
+
+// ---------------------------------------------------------------------------
+// Wide small-problem pass (packed d <= 3, log-sum-exp, no moment).
+//
+// One CTA of WTPB = 512 threads owns WROWS = 32 output rows -- lane l of every
+// warp holds row row_base + l -- and its column slice, split evenly over its
+// 16 warps. Each warp stages its own sub-slice, CHUNK columns at a time, in its
+// own 8 KB of shared memory and runs the fixed-reference loop (the online loop
+// on fallback) for its lane's row; the 16 partial (max, sum) pairs of a row are
+// merged in shared memory. A problem with few rows (n <= 32 x SMs) so fills the
+// GPU with whole rows per CTA: no column-split partials in global memory, no
+// tickets and no single merging CTA per row block, which dominate the
+// 128-row-block kernel at n = m = 4096. With P.splits > 1 (long rows) the CTAs
+// of a row block still merge through P.part as pair_pass_kernel does.
+constexpr int WTPB = 512;
+constexpr int WWARPS = WTPB / 32;
+constexpr int WROWS = 32;
+
+template <int PM, int D>
+__global__ void __launch_bounds__(WTPB, 1) pair_pass_wide_kernel(const __grid_constant__ PassParams P) {
+    extern __shared__ __align__(16) double smem[];   // WWARPS x CHUNK double4
+    __shared__ double sM[WWARPS][WROWS], sS[WWARPS][WROWS];
+    __shared__ double red[4 * WWARPS];
+    __shared__ int s_last;
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    Ctl *ctl = P.ctl;
+    if (ctl) {
+        if (ctl->stop) return;
+        if (P.gate == GATE_CHECK && !ctl->do_check) return;
+        if (P.gate == GATE_NOCHECK && ctl->do_check) return;
+    }
+    double alpha = 0.0, beta = 0.0;
+    resolve_coefs(P, alpha, beta);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rb = blockIdx.x, sp = blockIdx.y;
+    const int row_base = rb * WROWS;
+    const int o = row_base + lane;
+    const int cbeg = sp * P.cols_per_split;
+    const int cend = min(P.m, cbeg + P.cols_per_split);
+    // this warp's sub-slice, in whole 16-column chunks
+    int per = (cend - cbeg + WWARPS - 1) / WWARPS;
+    per = (per + 15) & ~15;
+    const int wb = min(cend, cbeg + warp * per), we = min(cend, wb + per);
+    double *wsm = smem + (size_t)warp * CHUNK * 4;
+
+    double Mv[1], Sv[1], Hv[1], MOMv[1] = {0.0};
+    // every warp reads the same rows' references, so the test agrees across warps
+    const bool fr = P.use_ref && __all_sync(0xffffffffu, o >= P.n || isfinite(row_reference(P, o, beta)));
+    bool good = false;
+    if (fr) good = __all_sync(0xffffffffu, tile_lse_fixedref<PM, D, 1, 32>(P, alpha, beta, row_base, wb, we,
+                                                                            wsm, Mv, Sv, Hv));
+    if (!good) tile_lse_packed<PM, D, 1, false, 2, 32>(P, alpha, beta, row_base, wb, we, wsm, Mv, Sv, MOMv, Hv);
+    sM[warp][lane] = Mv[0];
+    sS[warp][lane] = Sv[0];
+    __syncthreads();
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    if (warp == 0) {
+        double M = -INFINITY, S = 0.0, MO = 0.0;
+#pragma unroll 4
+        for (int w = 0; w < WWARPS; ++w) merge_lse(M, S, MO, sM[w][lane], sS[w][lane], 0.0);
+        Mv[0] = M;
+        Sv[0] = S;
+    }
+
+    if (P.splits > 1) {
+        // long rows: publish this slice's row totals; the last CTA of the row block merges
+        if (warp == 0 && o < P.n) {
+            double *pp = P.part + ((size_t)sp * P.n + o) * 3;
+            pp[0] = Mv[0];
+            pp[1] = Sv[0];
+        }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned t = atomicAdd(&P.rb_ticket[rb], 1u);
+            s_last = (t == (unsigned)(P.splits - 1));
+        }
+        __syncthreads();
+        if (!s_last) return;
+        __threadfence();
+        if (warp == 0 && o < P.n) {
+            double M = -INFINITY, S = 0.0, MO = 0.0;
+            for (int s2 = 0; s2 < P.splits; ++s2) {
+                const double *pp = P.part + ((size_t)s2 * P.n + o) * 3;
+                merge_lse(M, S, MO, __ldcg(pp), __ldcg(pp + 1), 0.0);
+            }
+            Mv[0] = M;
+            Sv[0] = S;
+        }
+        if (threadIdx.x == 0) P.rb_ticket[rb] = 0u;
+    }
+
+    if (fr) {
+        // lower side of the fixed-reference window on the merged row; a row whose
+        // LSE lies too far below its reference is recomputed over all columns
+        // with the online loop, split over the 16 warps
+        bool bad = false;
+        if (warp == 0 && o < P.n) {
+            const double mref = row_reference(P, o, beta) * LOG2E - Hv[0];
+            bad = !(Sv[0] > 0.0) || Mv[0] + log2(Sv[0]) < mref - fr_low_margin(P.m);
+        }
+        if (__syncthreads_or(bad)) {
+            int per2 = (P.m + WWARPS - 1) / WWARPS;
+            per2 = (per2 + 15) & ~15;
+            const int b2 = min(P.m, warp * per2), e2 = min(P.m, b2 + per2);
+            double M2[1], S2[1], H2[1], MO2[1] = {0.0};
+            tile_lse_packed<PM, D, 1, false, 2, 32>(P, alpha, beta, row_base, b2, e2, wsm, M2, S2, MO2, H2);
+            sM[warp][lane] = M2[0];
+            sS[warp][lane] = S2[0];
+            __syncthreads();
+            if (warp == 0) {
+                double M = -INFINITY, S = 0.0, MO = 0.0;
+                for (int w = 0; w < WWARPS; ++w) merge_lse(M, S, MO, sM[w][lane], sS[w][lane], 0.0);
+                Mv[0] = M;
+                Sv[0] = S;
+            }
+        }
+    }
+
+    row_epilogue<ACC_LSE, 1, WTPB>(P, rb, row_base, beta, Mv, Sv, MOMv, Hv, red, s_last, (int)gridDim.x, WROWS);
 }
 
 }  // namespace culamp_dev

@@ -37,13 +37,18 @@ def test_sinkhorn_cellsim_matches_oracle(oracle, metric):
     exact = oracle.np_cell_cost(a, metric)
     assert res.winf == pytest.approx(exact.max(), rel=1e-12)
     if p == 2.0:
-        cost = factor * oracle.feature_cost(pts, pts, 2)     # the BF16x3 inner products
-        tol_same, tol_exact = 1e-4, 5e-2
+        # the BF16x3 inner products; what remains is the FP32 (TMEM) accumulation
+        # of 64-term dot products of unit vectors, ~1e-6 relative, which the
+        # exponent scales by 1/(eta_p W_inf): 5e-5 of max |potential|
+        cost = factor * oracle.feature_cost(pts, pts, 2)
+        tol_same, tol_exact = None, 5e-2
     else:
         cost, tol_same, tol_exact = exact, 5e-6, 5e-6
     phi, psi, *_ = oracle.np_sinkhorn_kernel(pts, pts, r, c, 1e-2, 100, frequency=10, p=p, cost=cost,
                                              winf=res.winf)
     got_phi, got_psi = res.phi.cpu().numpy(), res.psi.cpu().numpy()
+    if tol_same is None:
+        tol_same = 5e-5 * np.abs(phi).max()
     assert np.abs(gauge(got_phi, r) - gauge(phi, r)).max() <= tol_same
     assert np.abs(gauge(got_psi, c) - gauge(psi, c)).max() <= tol_same
     phie, *_ = oracle.np_sinkhorn_kernel(pts, pts, r, c, 1e-2, 100, frequency=10, p=p, cost=exact,

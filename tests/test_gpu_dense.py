@@ -66,7 +66,9 @@ def test_sinkhorn_dense_matches_c_oracle(oracle, grid8, eta_p):
     got = np.array([row[1:6] for row in res.log])
     want = np.array([row[1:6] for row in log])
     assert got.shape == want.shape and np.array_equal(got[:, 0], want[:, 0])
-    np.testing.assert_allclose(got[:, 1], want[:, 1], rtol=1e-3, atol=1e-9)     # feas
+    # feas: within 1e-3 relative, or 2e-8 absolute where it approaches the floor
+    # of the FP32-exp iteration passes (~1e-7 relative log-sum-exp)
+    np.testing.assert_allclose(got[:, 1], want[:, 1], rtol=1e-3, atol=2e-8)
     np.testing.assert_allclose(got[:, 2:5], want[:, 2:5], rtol=1e-5, atol=1e-9)  # obj, primal, dual
     plan = _np(res.plan)
     want_plan = np.exp(-W / eta_p + phi[:, None] + psi[None, :])

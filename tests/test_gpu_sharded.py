@@ -107,14 +107,22 @@ def test_row_blocks_lamp_match_single_solver_and_oracle(oracle, p, eta_p, shards
     assert res.iterations == one.iterations == wst.iterations
     assert res.eta_t == one.eta_t == wst.eta_t
     got_nu = res.nu.cpu().numpy()
-    np.testing.assert_allclose(gauge(got_nu, c), gauge(one.nu.cpu().numpy(), c), atol=2e-6, rtol=0)
-    np.testing.assert_allclose(gauge(got_nu, c), gauge(nu, c), atol=2e-6, rtol=0)
-    np.testing.assert_allclose(res.theta.cpu().numpy(), theta, atol=5e-6, rtol=0)
+    # nu averages the theta iterates; the FP32-exp column sums of a different
+    # row split round differently (a few 1e-6 after 80 iterations)
+    np.testing.assert_allclose(gauge(got_nu, c), gauge(one.nu.cpu().numpy(), c), atol=5e-6, rtol=0)
+    np.testing.assert_allclose(gauge(got_nu, c), gauge(nu, c), atol=5e-6, rtol=0)
+    # theta's mirror step divides the column residual by eta_mu_j = (c_j + alpha/n) / tau_mu,
+    # about 1/m, so the ~1e-7 rounding of FP32-exp column sums reaches theta amplified
+    # by ~m (here 400): 5e-5
+    np.testing.assert_allclose(res.theta.cpu().numpy(), theta, atol=5e-5, rtol=0)
+    np.testing.assert_allclose(res.theta.cpu().numpy(), one.theta.cpu().numpy(), atol=5e-5, rtol=0)
     got = np.array(res.log)
     want = np.array([row[1:6] for row in log])
     assert got.shape == want.shape and np.array_equal(got[:, 0], want[:, 0])
     np.testing.assert_allclose(got[:, 1], want[:, 1], rtol=1e-3, atol=1e-9)
-    np.testing.assert_allclose(got[:, 2:], want[:, 2:], rtol=1e-4, atol=1e-6)
+    # objective, primal, dual: the dual is evaluated at theta, which carries the
+    # 5e-5 above
+    np.testing.assert_allclose(got[:, 2:], want[:, 2:], rtol=1e-4, atol=5e-5)
 
 
 def test_single_rank_nccl_group(tmp_path):
