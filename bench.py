@@ -27,6 +27,7 @@ import statistics
 import sys
 import threading
 import time
+import types
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "culamp.jl_b200"))
@@ -492,6 +493,18 @@ def main():
     return 0
 
 
+def form_leg(cb, X, Y, R, C, freq, flags, chosen):
+    """One Sinkhorn solve to EPS in another precision form, capped at three
+    times the chosen form's iterations, with its FP64 marginal re-check."""
+    a = cb.EOTArgs(eta_p=ETA, epsilon=EPS, itermax=3 * max(1, chosen.iterations), tmax=60.0,
+                   verbose=False)
+    s = cb.solve_sinkhorn(X, Y, R, C, a, freq, P, flags=flags, log_cap=100000)
+    rl, cl = cb.marginal_error_fp64(X, Y, R, C, s.phi, s.psi, ETA, s.winf, P)
+    return {"reached_tol": s.stopped == 1, "ms": s.elapsed_ms, "iterations": s.iterations,
+            "ms_per_iter": s.elapsed_ms / max(1, s.iterations), "fp64_row_l1": rl, "fp64_col_l1": cl,
+            "chosen_over_this": (s.elapsed_ms / chosen.elapsed_ms) if s.stopped == 1 else None}
+
+
 def extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_chosen, chosen_ms):
     """Chosen vs plain FP32 form, LAMP, and the 65536-point north-star solve."""
     ex = {}
@@ -505,6 +518,9 @@ def extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_chosen, chosen_ms):
         "iterations": pl.iterations, "ms_per_iter": pl.elapsed_ms / max(1, pl.iterations),
         "best_l1": best, "chosen_over_plain_speedup":
             (pl.elapsed_ms / chosen_ms) if pl.stopped == 1 else None}
+    chosen = types.SimpleNamespace(iterations=it_chosen, elapsed_ms=chosen_ms)
+    for name, fl in (("fp32_form", cb.FLAG_FORM_FP32), ("ladder", cb.FLAG_LADDER)):
+        ex[f"sinkhorn_{name}"] = form_leg(cb, X, Y, R, Cc, FREQ, fl, chosen)
     # LAMP (check every FREQ iterations, stop on the marginal test)
     b = cb.EOTArgs(eta_p=ETA, epsilon=EPS, itermax=100_000, tmax=60.0, verbose=False, B=1.1)
     fl = cb.FLAG_CHECK_ALWAYS | cb.FLAG_MARGINAL_ONLY
@@ -528,6 +544,9 @@ def extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_chosen, chosen_ms):
                             "iterations": s5.iterations, "fp64_row_l1": rl, "fp64_col_l1": cl,
                             "pass_ms": ms5, "pass_timing": how5,
                             "pass_gpair_s": 65536.0 ** 2 / (ms5 * 1e-3) / 1e9}
+    # the same engine with FP32 exponents, and the FP32 -> FP64 ladder
+    for name, fl in (("fp32_form", cb.FLAG_FORM_FP32), ("ladder", cb.FLAG_LADDER)):
+        ex[f"sinkhorn_65536_{name}"] = form_leg(cb, X5, Y5, R5, C5, 25, fl, s5)
     # the plain FP32 form on the same 65536-point instance (capped: it is not
     # expected to reach 1e-6), and LAMP to 1e-6 (marginal test every 25 iterations)
     ap = cb.EOTArgs(eta_p=ETA, epsilon=EPS, itermax=3 * s5.iterations, tmax=30.0, verbose=False)

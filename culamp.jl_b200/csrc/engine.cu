@@ -30,31 +30,11 @@ LaunchShape pass_shape(int n, int m, int d, int acc, int sm_count, bool mom) {
     LaunchShape s{};
     const bool packed = d >= 1 && d <= MAXD_PACKED;
     const int sms = sm_count > 0 ? sm_count : 148;
-    s.wide = false;
     // More rows per thread amortise each broadcast column over more pairs;
     // used when there are enough row blocks to fill the GPU with few column
     // splits. Measured (row pass, d = 3): 4 rows beat 8 by 16 % at 16384^2
     // (4 CTAs per SM instead of 3), 8 beat 4 by 4 % at 65536^2.
     const bool big = acc == ACC_LSE && packed && !mom;
-    // Few rows (at most one 32-row block per SM): the wide kernel keeps whole
-    // rows in one CTA and merges its 16 warps' column slices in shared memory;
-    // rows are split over CTAs only as far as needed to fill the SMs.
-    static const bool wide_off = std::getenv("CULAMP_NO_WIDE") != nullptr;
-    if (big && !wide_off && n <= WROWS * sms && m >= 1024) {
-        s.wide = true;
-        s.R = 1;
-        s.rb = (n + WROWS - 1) / WROWS;
-        int sp = sms / s.rb;
-        if (sp < 1) sp = 1;
-        int cps = (m + sp - 1) / sp;
-        cps = ((cps + 16 * WWARPS - 1) / (16 * WWARPS)) * (16 * WWARPS);
-        s.splits = (m + cps - 1) / cps;
-        s.cols_per_split = cps;
-        s.smem = (size_t)WWARPS * CHUNK * 4 * sizeof(double);
-        s.part_bytes = s.splits > 1 ? (size_t)s.splits * (size_t)n * 3 * sizeof(double) : 0;
-        s.sms = sms;
-        return s;
-    }
     s.R = (big && n >= 32768) ? RPT_BIG : ((big && n >= 16384) ? RPT_MID : RPT);
     const int rows = TPB * s.R;
     s.rb = (n + rows - 1) / rows;
@@ -114,7 +94,7 @@ static cudaError_t launch_any(const PassParams &P, int pm, int acc, const Launch
 
 cudaError_t launch_pass_at(PassParams P, int pm, int acc, const LaunchShape &sh, double *part,
                            unsigned *tickets, double *blk, cudaStream_t st) {
-    if (P.want_moment && (sh.R != RPT || sh.wide)) return cudaErrorInvalidValue;
+    if (P.want_moment && sh.R != RPT) return cudaErrorInvalidValue;
     P.splits = sh.splits;
     P.cols_per_split = sh.cols_per_split;
     P.part = part;
@@ -127,7 +107,7 @@ cudaError_t launch_pass_at(PassParams P, int pm, int acc, const LaunchShape &sh,
 cudaError_t launch_pass(PassParams P, int pm, int acc, const LaunchShape &sh, Scratch &scr,
                         cudaStream_t st) {
     if (P.fx) return launch_feat_pass(P, acc, scr, sh.sms, st);       // tensor-core feature path
-    if (P.want_moment && (sh.R != RPT || sh.wide)) return cudaErrorInvalidValue;   // shape built without mom
+    if (P.want_moment && sh.R != RPT) return cudaErrorInvalidValue;   // shape built without mom
     P.splits = sh.splits;
     P.cols_per_split = sh.cols_per_split;
     P.part = scr.part.as<double>();

@@ -90,8 +90,18 @@ enum Finish {
     FIN_SK_SYM = 9,      // symmetric Sinkhorn pass: tolerance test, iteration bookkeeping
 };
 
+// Precision ladder stall test: a check whose residual is not below this
+// fraction of the previous check's leaves the FP32-exponent phase. Sinkhorn at
+// eta_p = 1e-3 gains only ~7 % per 10 iterations, so the test is plain
+// non-decrease: at the FP32 floor the residual wanders up and down.
+constexpr double LADDER_STALL = 1.0;
+
 // Gate: when the kernel runs.
-enum Gate { GATE_ALWAYS = 0, GATE_CHECK = 1, GATE_NOCHECK = 2 };
+enum Gate {
+    GATE_ALWAYS = 0, GATE_CHECK = 1, GATE_NOCHECK = 2,
+    GATE_FP32 = 3,       // precision ladder: runs while ctl->fp32_phase is set
+    GATE_FP64 = 4,       // precision ladder: runs once ctl->fp32_phase is cleared
+};
 
 // Device-resident solver state. All fields written by device code are read by
 // later kernels only (stream order), never by concurrently running CTAs.
@@ -123,6 +133,9 @@ struct Ctl {
     culamp_log_row *log;
     double sums[4];             // FIN_SUMS output
     int error;                  // device-side error code (bounded waits etc.)
+    int fp32_phase;             // precision ladder: FP32-exponent iterations still active
+    double ladder_switch;       // ... until a check's L1 residual falls to this
+    double ladder_prev;         // the previous check's L1 residual (stall test)
     long long loops;            // WHILE-body executions (independent loop bound)
 };
 
@@ -151,6 +164,7 @@ struct PassParams {
     // moments
     int want_moment;            // 1: accumulate the softmax-weighted cost moment (MOM kernels)
     int use_ref;                // 1: fixed-reference fast path, reference = the row's previous LSE
+    int fp32;                   // 1 (with use_ref, p = 2, d <= 3): its exponent in FP32 (FORM_FP32)
     // gating and control
     int gate;
     int finish;
@@ -522,6 +536,12 @@ static __device__ __noinline__ void run_finish(const PassParams &P, const double
             const double l1 = tot[0];
             c->residual = l1;
             c->objective = tot[1];
+            // precision ladder: FP64 passes from here once the residual is near
+            // the tolerance, or once the FP32-exponent iteration stops gaining
+            // (its rounding floor lies above the tolerance)
+            if (c->fp32_phase && (l1 <= c->ladder_switch || l1 >= LADDER_STALL * c->ladder_prev))
+                c->fp32_phase = 0;
+            c->ladder_prev = l1;
             put_log(c, (double)c->iter, l1, tot[1], nan(""), c->dualval + tot[2]);
             if (l1 <= c->epsilon / 6.0) { c->stop = 1; c->stop_reason = 1; }
             else {
@@ -590,9 +610,7 @@ static __device__ __noinline__ void run_finish(const PassParams &P, const double
     }
 }
 
-// Block-wide FP64 sum of up to 4 values per thread (NT threads); result valid
-// in thread 0. red holds 4 * NT / 32 doubles.
-template <int NT = TPB>
+// Block-wide FP64 sum of up to 4 values per thread; result valid in thread 0.
 __device__ __forceinline__ void block_sum4(double (&v)[4], double *red) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -609,15 +627,14 @@ __device__ __forceinline__ void block_sum4(double (&v)[4], double *red) {
     if (threadIdx.x == 0) {
         for (int k = 0; k < 4; ++k) {
             double s = 0.0;
-            for (int ww = 0; ww < NT / 32; ++ww) s += red[ww * 4 + k];
+            for (int ww = 0; ww < TPB / 32; ++ww) s += red[ww * 4 + k];
             v[k] = s;
         }
     }
 }
 
 
-// Block-wide FP64 max of one value (NT threads); result valid in thread 0.
-template <int NT = TPB>
+// Block-wide FP64 max of one value; result valid in thread 0.
 __device__ __forceinline__ double block_max1(double x, double *red) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_down_sync(0xffffffffu, x, o));
@@ -626,7 +643,7 @@ __device__ __forceinline__ double block_max1(double x, double *red) {
     if (l == 0) red[w] = x;
     __syncthreads();
     if (threadIdx.x == 0)
-        for (int ww = 1; ww < NT / 32; ++ww) x = fmax(x, red[ww]);
+        for (int ww = 1; ww < TPB / 32; ++ww) x = fmax(x, red[ww]);
     return x;
 }
 
@@ -828,25 +845,15 @@ __device__ __forceinline__ void fr_col2(const double4 c0, const double4 c1, cons
     }
 }
 
-// Synchronises the threads that stage one column tile together: the CTA
-// (GT = TPB) or one warp (GT = 32, the wide small-problem pass).
-template <int GT>
-__device__ __forceinline__ void group_sync() {
-    if constexpr (GT == 32) __syncwarp();
-    else __syncthreads();
-}
-
 // Returns false when a real row's partial sum overflowed the window (a term
-// clamped high, or a non-finite input). GT threads (the CTA, or one warp)
-// share the staged column tile; thread g of the group owns rows
-// row_base + g + r * GT.
-template <int PM, int D, int R, int GT = TPB>
+// clamped high, or a non-finite input).
+template <int PM, int D, int R>
 __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double alpha, double beta,
                                                   int row_base, int cbeg, int cend, double *smem,
                                                   double (&Mo)[R], double (&So)[R],
                                                   double (&Ho)[R]) {
     constexpr bool SQ = (PM == P_SQ);
-    const int tid = threadIdx.x % GT;
+    const int tid = threadIdx.x;
     const double a2 = alpha * LOG2E;
     const double cb = P.colpot_unit ? LOG2E : beta * LOG2E;
     double ctr[D];
@@ -858,7 +865,7 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
     acc.zero();
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        const int row = row_base + tid + r * GT;
+        const int row = row_base + tid + r * TPB;
         const bool ok = row < P.n;
         double h = 0.0;
 #pragma unroll
@@ -873,8 +880,8 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
     }
     double4 *tile = reinterpret_cast<double4 *>(smem);
     for (int c0 = cbeg; c0 < cend; c0 += CHUNK) {
-        group_sync<GT>();
-        for (int q = tid; q < CHUNK; q += GT) {
+        __syncthreads();
+        for (int q = tid; q < CHUNK; q += TPB) {
             const int j = c0 + q;
             double4 v = make_double4(0.0, 0.0, 0.0, -INFINITY);
             if (j < cend) {
@@ -892,7 +899,7 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
             }
             tile[q] = v;
         }
-        group_sync<GT>();
+        __syncthreads();
         const int nc = min(CHUNK, cend - c0);
         int q = 0;
         // few rows per thread (small problems): unroll more columns so each warp
@@ -916,7 +923,7 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
     bool good = true;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        const int row = row_base + tid + r * GT;
+        const int row = row_base + tid + r * TPB;
         const bool real_row = row < P.n;
         double h = 0.0;
 #pragma unroll
@@ -935,16 +942,147 @@ __device__ __forceinline__ bool tile_lse_fixedref(const PassParams &P, double al
     return good;
 }
 
+// ---------------------------------------------------------------------------
+// FP32-exponent fixed-reference tile (CULAMP_FLAG_FORM_FP32): the same tiling,
+// reference and fallbacks as tile_lse_fixedref, but the exponent itself is
+// formed in FP32 -- the column term g_j and the row term (reference and |x|^2
+// part) are rounded to FP32 once, the d products are FP32 FMAs -- and 2^t goes
+// straight to the MUFU ex2 (no clamp: ex2 saturates to +inf above 128, which
+// the slice's sum check catches, and flushes to 0 below -126, which the
+// merged-row check bounds). Two rows share each packed FP32x2 FMA and add.
+// Per pair about 3.5 instructions and one MUFU op, against ~10 for the FP64
+// exponent; the FP32 rounding of terms of size |g| + |K| (up to ~1e4 log2
+// units at eta_p = 1e-3) limits each term to ~1e-4 relative, which is the
+// precision the plain FP32 form has.
+constexpr double FR32_LOW_MARGIN = 61.0;
+
+__device__ __forceinline__ unsigned long long fma_f32x2(unsigned long long a, unsigned long long b,
+                                                       unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+template <int PM, int D, int R>
+__device__ __forceinline__ bool tile_lse_fr32(const PassParams &P, double alpha, double beta,
+                                              int row_base, int cbeg, int cend, double *smem,
+                                              double (&Mo)[R], double (&So)[R], double (&Ho)[R]) {
+    static_assert(PM == P_SQ, "the FP32-exponent tile uses the |x|^2 + |y|^2 - 2 x.y expansion");
+    constexpr int NP = (R + 1) / 2;
+    const int tid = threadIdx.x;
+    const double a2 = alpha * LOG2E;
+    const double cb = P.colpot_unit ? LOG2E : beta * LOG2E;
+    double ctr[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) ctr[k] = P.ctr ? P.ctr[k] : 0.0;
+    unsigned long long xr2[NP][D], K2[NP];   // rows (2j, 2j+1) packed
+    float S[R], Cc[R];
+    unsigned long long acc[NP];
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+        float xv[2][D], kv[2];
+#pragma unroll
+        for (int h2 = 0; h2 < 2; ++h2) {
+            const int r = 2 * j + h2;
+            const int row = row_base + tid + r * TPB;
+            const bool ok = r < R && row < P.n;
+            double h = 0.0;
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                const double v = ok ? P.X[(size_t)row * D + k] - ctr[k] : 0.0;
+                xv[h2][k] = (float)(-2.0 * a2 * v);
+                h = fma(v, v, h);
+            }
+            // t - Mref = g_j + xr.y + (a2 |x|^2 - Mref)
+            const double m = ok ? row_reference(P, row, beta) * LOG2E : 0.0;
+            kv[h2] = ok ? (float)(a2 * h - m) : 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < D; ++k) xr2[j][k] = pack_f32x2(xv[0][k], xv[1][k]);
+        K2[j] = pack_f32x2(kv[0], kv[1]);
+        acc[j] = 0ull;
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) { S[r] = 0.f; Cc[r] = 0.f; }
+    float4 *tile = reinterpret_cast<float4 *>(smem);
+    for (int c0 = cbeg; c0 < cend; c0 += CHUNK) {
+        __syncthreads();
+        for (int q = tid; q < CHUNK; q += TPB) {
+            const int j = c0 + q;
+            float4 v = make_float4(0.f, 0.f, 0.f, -INFINITY);
+            if (j < cend) {
+                double yy[3] = {0.0, 0.0, 0.0};
+                double s2 = 0.0;
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+                    yy[k] = P.Y[(size_t)j * D + k] - ctr[k];
+                    s2 = fma(yy[k], yy[k], s2);
+                }
+                const double pot = P.colpot ? P.colpot[j] : 0.0;
+                const double g = ((cb == 0.0) ? 0.0 : cb * pot) + a2 * s2;
+                v = make_float4((float)yy[0], (float)yy[1], (float)yy[2], (float)g);
+            }
+            tile[q] = v;
+        }
+        __syncthreads();
+        const int nc = min(CHUNK, cend - c0);
+        for (int q0 = 0; q0 < nc; q0 += 16) {
+            const int q1 = min(nc, q0 + 16);
+#pragma unroll 4
+            for (int q = q0; q < q1; ++q) {
+                const float4 col = tile[q];
+                const unsigned long long g2 = pack_f32x2(col.w, col.w);
+                const unsigned long long y0 = pack_f32x2(col.x, col.x);
+                const unsigned long long y1 = pack_f32x2(col.y, col.y);
+                const unsigned long long y2 = pack_f32x2(col.z, col.z);
+#pragma unroll
+                for (int j = 0; j < NP; ++j) {
+                    unsigned long long t = add_f32x2(g2, K2[j]);
+                    if (D >= 3) t = fma_f32x2(xr2[j][D >= 3 ? 2 : 0], y2, t);
+                    if (D >= 2) t = fma_f32x2(xr2[j][D >= 2 ? 1 : 0], y1, t);
+                    t = fma_f32x2(xr2[j][0], y0, t);
+                    const float e0 = ex2_approx(lo_f32(t));
+                    const float e1 = (2 * j + 1 < R) ? ex2_approx(hi_f32(t)) : 0.f;
+                    acc[j] = add_f32x2(acc[j], pack_f32x2(e0, e1));
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < NP; ++j) {
+                kahan_add(S[2 * j], Cc[2 * j], lo_f32(acc[j]));
+                if (2 * j + 1 < R) kahan_add(S[2 * j + 1], Cc[2 * j + 1], hi_f32(acc[j]));
+                acc[j] = 0ull;
+            }
+        }
+    }
+    bool good = true;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int row = row_base + tid + r * TPB;
+        const bool real_row = row < P.n;
+        double h = 0.0;
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            const double v = real_row ? P.X[(size_t)row * D + k] - ctr[k] : 0.0;
+            h = fma(v, v, h);
+        }
+        Ho[r] = a2 * h;
+        Mo[r] = (real_row ? row_reference(P, row, beta) * LOG2E : 0.0) - Ho[r];
+        const double sv = (double)S[r] - (double)Cc[r];
+        So[r] = sv;
+        if (real_row && !(sv <= 0x1p64)) good = false;
+    }
+    return good;
+}
+
 // Packed (d <= 3) log-sum-exp tile: rows in registers, column tiles of CHUNK
-// (y - ctr, g) double4 entries in shared memory, broadcast to the warp. GT
-// threads share the staged tile, as in tile_lse_fixedref.
-template <int PM, int D, int R, bool MOM, int UNROLL = 8, int GT = TPB>
+// (y - ctr, g) double4 entries in shared memory, broadcast to the warp.
+template <int PM, int D, int R, bool MOM, int UNROLL = 8>
 __device__ __forceinline__ void tile_lse_packed(const PassParams &P, double alpha, double beta,
                                                 int row_base, int cbeg, int cend, double *smem,
                                                 double (&Mo)[R], double (&So)[R],
                                                 double (&MOMo)[R], double (&Ho)[R]) {
     constexpr bool SQ = (PM == P_SQ);
-    const int tid = threadIdx.x % GT;
+    const int tid = threadIdx.x;
     const double a2 = alpha * LOG2E;
     const double cb = P.colpot_unit ? LOG2E : beta * LOG2E;
     double ctr[D];
@@ -956,7 +1094,7 @@ __device__ __forceinline__ void tile_lse_packed(const PassParams &P, double alph
     float S[R], Cc[R], cs[R], mo[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        const int row = row_base + tid + r * GT;
+        const int row = row_base + tid + r * TPB;
         const bool ok = row < P.n;
         double h = 0.0;
 #pragma unroll
@@ -972,8 +1110,8 @@ __device__ __forceinline__ void tile_lse_packed(const PassParams &P, double alph
     }
     double4 *tile = reinterpret_cast<double4 *>(smem);
     for (int c0 = cbeg; c0 < cend; c0 += CHUNK) {
-        group_sync<GT>();
-        for (int q = tid; q < CHUNK; q += GT) {
+        __syncthreads();
+        for (int q = tid; q < CHUNK; q += TPB) {
             const int j = c0 + q;
             double4 v = make_double4(0.0, 0.0, 0.0, -INFINITY);
             if (j < cend) {
@@ -991,7 +1129,7 @@ __device__ __forceinline__ void tile_lse_packed(const PassParams &P, double alph
             }
             tile[q] = v;
         }
-        group_sync<GT>();
+        __syncthreads();
         const int nc = min(CHUNK, cend - c0);
         int q = 0;
         for (; q + 8 <= nc; q += 8) {
@@ -1013,13 +1151,12 @@ __device__ __forceinline__ void tile_lse_packed(const PassParams &P, double alph
 }
 
 // Per-row epilogue of a reduction pass (one thread per output row, R rows per
-// thread, NT threads of which the first `rows_blk` / R own rows) and the
-// grid-level finish step run by the last CTA of the grid.
-template <int ACC, int R, int NT = TPB>
+// thread) and the grid-level finish step run by the last CTA of the grid.
+template <int ACC, int R>
 __device__ __forceinline__ void row_epilogue(const PassParams &P, int rb, int row_base, double beta,
                                              const double (&Mv)[R], const double (&Sv)[R],
                                              const double (&MOMv)[R], const double (&Hv)[R],
-                                             double *red, int &s_last, int nrb, int rows_blk = NT * R) {
+                                             double *red, int &s_last, int nrb) {
     Ctl *ctl = P.ctl;
     double acc4[4] = {0.0, 0.0, 0.0, 0.0};
     double amax = -INFINITY;
@@ -1028,9 +1165,8 @@ __device__ __forceinline__ void row_epilogue(const PassParams &P, int rb, int ro
     else if (P.lamp_step == LAMP_B) en = ctl->eta_next;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        const int lo = threadIdx.x + r * NT;
-        const int o = row_base + lo;
-        if (o >= P.n || lo >= rows_blk) continue;
+        const int o = row_base + threadIdx.x + r * TPB;
+        if (o >= P.n) continue;
         if (ACC != ACC_LSE) {
             if (P.out) P.out[o] = Mv[r];
             amax = fmax(amax, Mv[r]);
@@ -1108,10 +1244,10 @@ __device__ __forceinline__ void row_epilogue(const PassParams &P, int rb, int ro
 
     if (P.finish == FIN_NONE) return;
     if (ACC == ACC_MAX) {
-        const double bm = block_max1<NT>(amax, red);
+        const double bm = block_max1(amax, red);
         acc4[0] = bm;
     } else {
-        block_sum4<NT>(acc4, red);
+        block_sum4(acc4, red);
     }
     if (threadIdx.x == 0) {
         for (int k = 0; k < 4; ++k) P.blk[rb * 4 + k] = acc4[k];
@@ -1143,7 +1279,9 @@ __device__ __forceinline__ void row_epilogue(const PassParams &P, int rb, int ro
 // CTA b belongs to the instance i with block_start[i] <= b < block_start[i+1]
 // and is its local block b - block_start[i] = sp * nrb + rb. Each instance
 // carries its own parameters (plist[i]), scratch, tickets and control block.
-template <int PM, int D, int ACC, int R, bool MOM, bool FR, bool BAT = false>
+// F32: the fixed-reference loop forms the exponent in FP32 (tile_lse_fr32,
+// CULAMP_FLAG_FORM_FP32); its fallbacks stay FP64.
+template <int PM, int D, int ACC, int R, bool MOM, bool FR, bool BAT = false, bool F32 = false>
 __global__ void __launch_bounds__(TPB, (R > RPT_MID) ? 3 : 4)
     pair_pass_kernel(const __grid_constant__ PassParams P0, const PassParams *plist,
                      const int *block_start, int count) {
@@ -1187,6 +1325,8 @@ __global__ void __launch_bounds__(TPB, (R > RPT_MID) ? 3 : 4)
         if (ctl->stop) return;
         if (P.gate == GATE_CHECK && !ctl->do_check) return;
         if (P.gate == GATE_NOCHECK && ctl->do_check) return;
+        if (P.gate == GATE_FP32 && !ctl->fp32_phase) return;
+        if (P.gate == GATE_FP64 && ctl->fp32_phase) return;
     }
     double alpha = 0.0, beta = 0.0;
     if (ACC == ACC_LSE) resolve_coefs(P, alpha, beta);
@@ -1213,8 +1353,11 @@ __global__ void __launch_bounds__(TPB, (R > RPT_MID) ? 3 : 4)
                     fr_tried = true;
 #pragma unroll
                     for (int r = 0; r < R; ++r) MOMv[r] = 0.0;
-                    const bool good = tile_lse_fixedref<PM, D, R>(P, alpha, beta, row_base, cbeg, cend,
-                                                                  smem, Mv, Sv, Hv);
+                    bool good;
+                    if constexpr (F32 && PM == P_SQ)
+                        good = tile_lse_fr32<PM, D, R>(P, alpha, beta, row_base, cbeg, cend, smem, Mv, Sv, Hv);
+                    else
+                        good = tile_lse_fixedref<PM, D, R>(P, alpha, beta, row_base, cbeg, cend, smem, Mv, Sv, Hv);
                     done = !__syncthreads_or(!good);
                 }
             }
@@ -1289,7 +1432,7 @@ __global__ void __launch_bounds__(TPB, (R > RPT_MID) ? 3 : 4)
         // terms could matter and the row block is recomputed over all columns.
         if (fr_tried) {
             const double a2 = alpha * LOG2E;
-            const double margin = fr_low_margin(P.m);
+            const double margin = F32 ? FR32_LOW_MARGIN : fr_low_margin(P.m);
             bool bad = false;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -1308,127 +1451,6 @@ __global__ void __launch_bounds__(TPB, (R > RPT_MID) ? 3 : 4)
 #undef CULAMP_RB
 #undef CULAMP_SP
 #undef CULAMP_NRB
-}
-
-// ---------------------------------------------------------------------------
-// Wide small-problem pass (packed d <= 3, log-sum-exp, no moment).
-//
-// One CTA of WTPB = 512 threads owns WROWS = 32 output rows -- lane l of every
-// warp holds row row_base + l -- and its column slice, split evenly over its
-// 16 warps. Each warp stages its own sub-slice, CHUNK columns at a time, in its
-// own 8 KB of shared memory and runs the fixed-reference loop (the online loop
-// on fallback) for its lane's row; the 16 partial (max, sum) pairs of a row are
-// merged in shared memory. A problem with few rows (n <= 32 x SMs) so fills the
-// GPU with whole rows per CTA: no column-split partials in global memory, no
-// tickets and no single merging CTA per row block, which dominate the
-// 128-row-block kernel at n = m = 4096. With P.splits > 1 (long rows) the CTAs
-// of a row block still merge through P.part as pair_pass_kernel does.
-constexpr int WTPB = 512;
-constexpr int WWARPS = WTPB / 32;
-constexpr int WROWS = 32;
-
-template <int PM, int D>
-__global__ void __launch_bounds__(WTPB, 1) pair_pass_wide_kernel(const __grid_constant__ PassParams P) {
-    extern __shared__ __align__(16) double smem[];   // WWARPS x CHUNK double4
-    __shared__ double sM[WWARPS][WROWS], sS[WWARPS][WROWS];
-    __shared__ double red[4 * WWARPS];
-    __shared__ int s_last;
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    Ctl *ctl = P.ctl;
-    if (ctl) {
-        if (ctl->stop) return;
-        if (P.gate == GATE_CHECK && !ctl->do_check) return;
-        if (P.gate == GATE_NOCHECK && ctl->do_check) return;
-    }
-    double alpha = 0.0, beta = 0.0;
-    resolve_coefs(P, alpha, beta);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int rb = blockIdx.x, sp = blockIdx.y;
-    const int row_base = rb * WROWS;
-    const int o = row_base + lane;
-    const int cbeg = sp * P.cols_per_split;
-    const int cend = min(P.m, cbeg + P.cols_per_split);
-    // this warp's sub-slice, in whole 16-column chunks
-    int per = (cend - cbeg + WWARPS - 1) / WWARPS;
-    per = (per + 15) & ~15;
-    const int wb = min(cend, cbeg + warp * per), we = min(cend, wb + per);
-    double *wsm = smem + (size_t)warp * CHUNK * 4;
-
-    double Mv[1], Sv[1], Hv[1], MOMv[1] = {0.0};
-    // every warp reads the same rows' references, so the test agrees across warps
-    const bool fr = P.use_ref && __all_sync(0xffffffffu, o >= P.n || isfinite(row_reference(P, o, beta)));
-    bool good = false;
-    if (fr) good = __all_sync(0xffffffffu, tile_lse_fixedref<PM, D, 1, 32>(P, alpha, beta, row_base, wb, we,
-                                                                            wsm, Mv, Sv, Hv));
-    if (!good) tile_lse_packed<PM, D, 1, false, 2, 32>(P, alpha, beta, row_base, wb, we, wsm, Mv, Sv, MOMv, Hv);
-    sM[warp][lane] = Mv[0];
-    sS[warp][lane] = Sv[0];
-    __syncthreads();
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    if (warp == 0) {
-        double M = -INFINITY, S = 0.0, MO = 0.0;
-#pragma unroll 4
-        for (int w = 0; w < WWARPS; ++w) merge_lse(M, S, MO, sM[w][lane], sS[w][lane], 0.0);
-        Mv[0] = M;
-        Sv[0] = S;
-    }
-
-    if (P.splits > 1) {
-        // long rows: publish this slice's row totals; the last CTA of the row block merges
-        if (warp == 0 && o < P.n) {
-            double *pp = P.part + ((size_t)sp * P.n + o) * 3;
-            pp[0] = Mv[0];
-            pp[1] = Sv[0];
-        }
-        __threadfence();
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const unsigned t = atomicAdd(&P.rb_ticket[rb], 1u);
-            s_last = (t == (unsigned)(P.splits - 1));
-        }
-        __syncthreads();
-        if (!s_last) return;
-        __threadfence();
-        if (warp == 0 && o < P.n) {
-            double M = -INFINITY, S = 0.0, MO = 0.0;
-            for (int s2 = 0; s2 < P.splits; ++s2) {
-                const double *pp = P.part + ((size_t)s2 * P.n + o) * 3;
-                merge_lse(M, S, MO, __ldcg(pp), __ldcg(pp + 1), 0.0);
-            }
-            Mv[0] = M;
-            Sv[0] = S;
-        }
-        if (threadIdx.x == 0) P.rb_ticket[rb] = 0u;
-    }
-
-    if (fr) {
-        // lower side of the fixed-reference window on the merged row; a row whose
-        // LSE lies too far below its reference is recomputed over all columns
-        // with the online loop, split over the 16 warps
-        bool bad = false;
-        if (warp == 0 && o < P.n) {
-            const double mref = row_reference(P, o, beta) * LOG2E - Hv[0];
-            bad = !(Sv[0] > 0.0) || Mv[0] + log2(Sv[0]) < mref - fr_low_margin(P.m);
-        }
-        if (__syncthreads_or(bad)) {
-            int per2 = (P.m + WWARPS - 1) / WWARPS;
-            per2 = (per2 + 15) & ~15;
-            const int b2 = min(P.m, warp * per2), e2 = min(P.m, b2 + per2);
-            double M2[1], S2[1], H2[1], MO2[1] = {0.0};
-            tile_lse_packed<PM, D, 1, false, 2, 32>(P, alpha, beta, row_base, b2, e2, wsm, M2, S2, MO2, H2);
-            sM[warp][lane] = M2[0];
-            sS[warp][lane] = S2[0];
-            __syncthreads();
-            if (warp == 0) {
-                double M = -INFINITY, S = 0.0, MO = 0.0;
-                for (int w = 0; w < WWARPS; ++w) merge_lse(M, S, MO, sM[w][lane], sS[w][lane], 0.0);
-                Mv[0] = M;
-                Sv[0] = S;
-            }
-        }
-    }
-
-    row_epilogue<ACC_LSE, 1, WTPB>(P, rb, row_base, beta, Mv, Sv, MOMv, Hv, red, s_last, (int)gridDim.x, WROWS);
 }
 
 }  // namespace culamp_dev

@@ -11,9 +11,9 @@ namespace culamp_host {
 
 using namespace culamp_dev;
 
-template <int PM, int D, int ACC, int R, bool MOM, bool FR = false>
+template <int PM, int D, int ACC, int R, bool MOM, bool FR = false, bool F32 = false>
 inline cudaError_t launch_t(const PassParams &P, const LaunchShape &sh, cudaStream_t st) {
-    auto kern = pair_pass_kernel<PM, D, ACC, R, MOM, FR>;
+    auto kern = pair_pass_kernel<PM, D, ACC, R, MOM, FR, false, F32>;
     if (sh.smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)sh.smem);
@@ -37,32 +37,18 @@ inline cudaError_t launch_t(const PassParams &P, const LaunchShape &sh, cudaStre
     return cudaGetLastError();
 }
 
-template <int PM, int D>
-inline cudaError_t launch_wide(const PassParams &P, const LaunchShape &sh, cudaStream_t st) {
-    auto kern = pair_pass_wide_kernel<PM, D>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem);
-    if (e != cudaSuccess) return e;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(sh.rb, sh.splits);
-    cfg.blockDim = dim3(WTPB);
-    cfg.dynamicSmemBytes = sh.smem;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = pdl_launches() ? 1 : 0;
-    e = cudaLaunchKernelEx(&cfg, kern, P);
-    if (e != cudaSuccess) return e;
-    return cudaGetLastError();
-}
-
 template <int PM, int D, int ACC>
 inline cudaError_t launch_v(const PassParams &P, const LaunchShape &sh, cudaStream_t st) {
     if constexpr (ACC == ACC_LSE) {
         if (P.want_moment) return launch_t<PM, D, ACC, RPT, true>(P, sh, st);
         if constexpr (D > 0) {
-            if (sh.wide) return launch_wide<PM, D>(P, sh, st);
+            if constexpr (PM == P_SQ) {
+                if (P.use_ref && P.fp32) {
+                    if (sh.R == RPT_BIG) return launch_t<PM, D, ACC, RPT_BIG, false, true, true>(P, sh, st);
+                    if (sh.R == RPT_MID) return launch_t<PM, D, ACC, RPT_MID, false, true, true>(P, sh, st);
+                    return launch_t<PM, D, ACC, RPT, false, true, true>(P, sh, st);
+                }
+            }
             if (P.use_ref) {
                 if (sh.R == RPT_BIG) return launch_t<PM, D, ACC, RPT_BIG, false, true>(P, sh, st);
                 if (sh.R == RPT_MID) return launch_t<PM, D, ACC, RPT_MID, false, true>(P, sh, st);

@@ -102,16 +102,16 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Wait for the phase with the given parity; false after FT_WAIT_NS (the abort
+// Wait for the phase with the given parity; false after limit_ns (the abort
 // flag is then set) or, when honor_abort, as soon as another role aborted.
 __device__ __noinline__ bool ft_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag,
-                                     bool honor_abort) {
+                                     bool honor_abort, unsigned long long limit_ns = FT_WAIT_NS) {
     if (mbar_try(bar, parity)) return true;
     const unsigned long long t0 = globaltimer_ns();
     for (;;) {
         if (mbar_try(bar, parity)) return true;
         if (honor_abort && *abort_flag) return false;
-        if (globaltimer_ns() - t0 > FT_WAIT_NS) {
+        if (globaltimer_ns() - t0 > limit_ns) {
             *abort_flag = 1;
             return false;
         }
@@ -761,3 +761,51 @@ cudaError_t launch_feat_batched(int np, int acc, bool mom, const PassParams *pli
 }
 
 }  // namespace culamp_host
+
+// ---------------------------------------------------------------------------
+// Probe of the bounded wait above: one CTA waits, with the given limit, on an
+// mbarrier phase that nothing completes (no thread arrives, no copy is
+// issued), so the wait must give up, set the abort flag and return -- the
+// path every role of feat_reduce_kernel takes when a copy or an MMA never
+// completes. The host reads the outcome; the context stays usable.
+namespace {
+__global__ void wait_probe_kernel(unsigned long long limit_ns, int *out) {
+    __shared__ __align__(8) unsigned long long bar;
+    __shared__ int abort_flag;
+    const uint32_t b = smem_u32(&bar);
+    if (threadIdx.x == 0) {
+        mbar_init(b, 1);
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    bool ok = true;
+    if (threadIdx.x == 0) ok = ft_wait(b, 0u, &abort_flag, false, limit_ns);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        out[0] = ok ? 0 : 1;
+        out[1] = abort_flag;
+    }
+}
+}  // namespace
+
+extern "C" int culamp_probe_wait(culamp_handle h, uint64_t limit_ns, void *stream) {
+    if (!h) return CULAMP_ERR_INVALID_ARG;
+    if (limit_ns == 0 || limit_ns > 10000000000ull)
+        return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "wait limit must be in (0, 10 s]");
+    cudaSetDevice(h->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (h->tmpA.reserve(2 * sizeof(int)) != cudaSuccess)
+        return culamp_set_error(h, CULAMP_ERR_ALLOC, "probe buffer");
+    int *dev = h->tmpA.as<int>();
+    wait_probe_kernel<<<1, 32, 0, st>>>((unsigned long long)limit_ns, dev);
+    int out[2] = {-1, -1};
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(out, dev, sizeof(out), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return culamp_set_error(h, CULAMP_ERR_CUDA, "wait probe failed");
+    if (out[0] == 1 && out[1] == 1)
+        return culamp_set_error(h, CULAMP_ERR_DEVICE_TIMEOUT, "bounded wait gave up after %llu ns",
+                                (unsigned long long)limit_ns);
+    return culamp_set_error(h, CULAMP_ERR_CUDA, "bounded wait did not give up (%d, %d)", out[0], out[1]);
+}

@@ -64,7 +64,6 @@ struct LaunchShape {
     size_t smem;       // dynamic shared memory bytes
     size_t part_bytes; // split scratch bytes
     int sms;           // SM count the shape was made for
-    bool wide;         // pair_pass_wide_kernel: 32 rows per 512-thread CTA
 };
 
 // Grid and scratch requirement of a pass over n output rows and m columns.

@@ -65,11 +65,13 @@ enum SolverKind { KIND_SK = 1, KIND_LAMP = 2, KIND_SYM = 3 };
 // Everything a captured graph bakes into kernel parameters.
 struct GraphKey {
     int kind = 0, n = 0, m = 0, d = 0, pm_iter = 0, pm_resid = 0, unroll = 0, feat = 0;
+    int form = 0;         // 0 FP64 exponent, 1 FP32 exponent, 2 precision ladder
     long long freq = 0;   // check cadence the body is aligned to (0: gated checks)
     double p = 0, winf = 0, B = 0, eta_mu = 0;
     long long generation = -1;
     bool operator==(const GraphKey &o) const {
         return kind == o.kind && n == o.n && m == o.m && d == o.d && pm_iter == o.pm_iter && feat == o.feat &&
+               form == o.form &&
                freq == o.freq &&
                pm_resid == o.pm_resid && unroll == o.unroll && generation == o.generation &&
                std::memcmp(&p, &o.p, sizeof(double)) == 0 && std::memcmp(&winf, &o.winf, sizeof(double)) == 0 &&
@@ -427,9 +429,16 @@ int copy_log(culamp_handle h, const Ctl &c, culamp_log_row *log, int64_t log_cap
 
 struct SkPlan {
     PassParams k1, k2, k3;
+    PassParams k1f, k2f;   // precision ladder: the FP32-exponent row / column passes
+    bool ladder = false;
     int pm_iter, pm_resid;
     LaunchShape s_rows, s_cols, s_rows_mom;
 };
+
+// The FP32-exponent forms (FORM_FP32, LADDER) exist for the packed p = 2 passes.
+bool fp32_form_applies(const Solver &S, int d, int pm_iter) {
+    return pm_iter == P_SQ && d <= MAXD_PACKED && !S.feat_active;
+}
 
 SkPlan make_sk_plan(culamp_handle h, int n, int m, int d, double p, uint32_t flags) {
     Solver &S = *h->solver;
@@ -477,6 +486,20 @@ SkPlan make_sk_plan(culamp_handle h, int n, int m, int d, double p, uint32_t fla
     apply_feat(S, pl.k1, true);
     apply_feat(S, pl.k2, false);
     apply_feat(S, pl.k3, true);
+    if (fp32_form_applies(S, d, pl.pm_iter)) {
+        if (flags & CULAMP_FLAG_FORM_FP32) {
+            pl.k1.fp32 = 1;
+            pl.k2.fp32 = 1;
+        } else if (flags & CULAMP_FLAG_LADDER) {
+            // FP32-exponent passes while ctl->fp32_phase holds, FP64 ones after
+            pl.ladder = true;
+            pl.k1f = pl.k1;
+            pl.k2f = pl.k2;
+            pl.k1f.fp32 = pl.k2f.fp32 = 1;
+            pl.k1f.gate = pl.k2f.gate = GATE_FP32;
+            pl.k1.gate = pl.k2.gate = GATE_FP64;
+        }
+    }
     pl.s_rows = pass_shape(n, m, d, ACC_LSE, h->sm_count);
     pl.s_cols = pass_shape(m, n, d, ACC_LSE, h->sm_count);
     pl.s_rows_mom = pass_shape(n, m, d, ACC_LSE, h->sm_count, true);
@@ -500,9 +523,15 @@ int sinkhorn_loop(culamp_handle h, int n, int m, int d, double p, double eta, do
     c.winf = winf;
     c.log = S.logbuf.as<culamp_log_row>();
     c.log_cap = log_cap;
+    SkPlan pl = make_sk_plan(h, n, m, d, p, flags);
+    // precision ladder: FP32-exponent iterations until a check's L1 residual is
+    // within LADDER_FACTOR of the stopping threshold, then the FP64 form
+    constexpr double LADDER_FACTOR = 32.0;
+    c.fp32_phase = pl.ladder ? 1 : 0;
+    c.ladder_switch = LADDER_FACTOR * args->epsilon / 6.0;
+    c.ladder_prev = INFINITY;
     CUDA_TRY(h, cudaMemcpyAsync(S.ctl.ptr, &c, sizeof(Ctl), cudaMemcpyHostToDevice, st));
     set_start_kernel<<<1, 1, 0, st>>>(S.ctl.as<Ctl>());
-    SkPlan pl = make_sk_plan(h, n, m, d, p, flags);
     // Graph bodies hold whole multiples of `frequency` iterations when the
     // cadence is short: every body then starts at a check iteration
     // ((it - 1) % frequency == 0, SinkhornKernel.jl:527), so the residual pass
@@ -512,7 +541,10 @@ int sinkhorn_loop(culamp_handle h, int n, int m, int d, double p, double eta, do
     const int unroll = aligned ? (int)frequency * std::max(1, (int)std::lround((double)base_unroll / frequency))
                                : base_unroll;
     auto iteration = [&](cudaStream_t s, bool with_check) -> cudaError_t {
-        cudaError_t e = launch_pass(pl.k1, pl.pm_iter, ACC_LSE, pl.s_rows, S.scr, s);
+        cudaError_t e = cudaSuccess;
+        if (pl.ladder) e = launch_pass(pl.k1f, pl.pm_iter, ACC_LSE, pl.s_rows, S.scr, s);
+        if (e == cudaSuccess) e = launch_pass(pl.k1, pl.pm_iter, ACC_LSE, pl.s_rows, S.scr, s);
+        if (e == cudaSuccess && pl.ladder) e = launch_pass(pl.k2f, pl.pm_iter, ACC_LSE, pl.s_cols, S.scr, s);
         if (e == cudaSuccess) e = launch_pass(pl.k2, pl.pm_iter, ACC_LSE, pl.s_cols, S.scr, s);
         if (e == cudaSuccess && with_check) e = launch_pass(pl.k3, pl.pm_resid, ACC_LSE, pl.s_rows_mom, S.scr, s);
         return e;
@@ -543,6 +575,7 @@ int sinkhorn_loop(culamp_handle h, int n, int m, int d, double p, double eta, do
         key.unroll = unroll;
         key.freq = aligned ? frequency : 0;
         key.generation = S.generation;
+        key.form = pl.ladder ? 2 : (pl.k1.fp32 ? 1 : 0);
         cudaGraphExec_t ex = nullptr;
         int s = get_graph(h, key, body, &ex, [&body_pos]() { body_pos = 0; });
         if (s) return s;

@@ -29,6 +29,8 @@ FLAG_FORM_PLAIN = 8
 FLAG_NO_GRAPH = 16
 FLAG_FEAT_X6 = 32
 FLAG_FEAT_FP64 = 64
+FLAG_FORM_FP32 = 128
+FLAG_LADDER = 256
 
 
 class CulampError(RuntimeError):
@@ -120,6 +122,7 @@ SIGNATURES = {
                                    _D, _U32, _VP, _VP, _VP, _VP, C.POINTER(CStats),
                                    C.POINTER(CLogRow), _I64]),
     "culamp_probe_pipes": (C.c_int, [_VP, C.POINTER(_D), _VP]),
+    "culamp_probe_wait": (C.c_int, [_VP, C.c_uint64, _VP]),
     "culamp_adjoint_sk": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, _D, _D, _D,
                                     _VP]),
     "culamp_lse_rows_sk_noalloc": (C.c_int, [_VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, _D, _D, _D,

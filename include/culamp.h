@@ -54,6 +54,14 @@ extern "C" {
 #define CULAMP_FLAG_FEAT_X6       32u  /* feature clouds (d >= 32, squared cost): BF16x6
                                           split products (3 bf16 pieces, ~24-bit products)
                                           instead of the default BF16x3 (2 pieces)          */
+#define CULAMP_FLAG_FORM_FP32    128u  /* Sinkhorn, p = 2, d <= 3: the chosen form's engine with the
+                                          exponent formed in FP32 (same tiling, reference,
+                                          graph loop; ~1e-4 relative per term)               */
+#define CULAMP_FLAG_LADDER       256u  /* Sinkhorn, p = 2, d <= 3: FP32-exponent iterations until
+                                          a check's L1 residual falls to 32 x epsilon/6 or
+                                          stops falling (not below the previous check's),
+                                          then the FP64-exponent form to the tolerance. The
+                                          check passes are FP64 in every form.              */
 #define CULAMP_FLAG_FEAT_FP64     64u  /* feature clouds on the FP64 pair loops instead of
                                           the tensor cores (exact inner products, slow)     */
 
@@ -362,6 +370,13 @@ int culamp_lse_rows_sk_noalloc(double *out, const double *x, const double *y, in
  * instruction rates that bound the pair passes: out[0] = DFMA/s, out[1] = MUFU
  * ex2/s, out[2] = FP64->FP32 conversions/s, out[3] = SM count. Synchronous. */
 int culamp_probe_pipes(culamp_handle h, double *out, void *stream);
+
+/* No counterpart in the reference. Runs the tensor-core path's bounded
+ * mbarrier wait (the one every role of the feature pass uses) on a barrier
+ * phase that nothing completes, with the given limit in ns (at most 10 s).
+ * Returns CULAMP_ERR_DEVICE_TIMEOUT when the wait gave up and reported it, as
+ * it must; the device context stays usable. Synchronous. */
+int culamp_probe_wait(culamp_handle h, uint64_t limit_ns, void *stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,116 @@
+"""The FP32-exponent form and the FP32 -> FP64 precision ladder of Sinkhorn
+(SinkhornKernel.jl:477-559, p = 2, d <= 3) on the 64x64-grid workload.
+
+* CULAMP_FLAG_FORM_FP32 runs the chosen form's engine (tiling, fixed row
+  reference, graph loop) with every exponent formed in FP32. Its check passes
+  stay FP64, so its logged L1 residuals are exact for the potentials it
+  reached. At a fixed iteration count its potentials follow the FP64-exponent
+  form within the FP32 rounding of the exponent (~|g| 2^-24 per term, |g|
+  up to ~1e3 in log2 units at eta_p = 1e-3): checked at 1e-4 of max |phi|
+  after removing the Sinkhorn gauge.
+* CULAMP_FLAG_LADDER switches from FP32 to FP64 passes on the device; the
+  solve stops on the FP64 check only, so the bench workload's 1e-6 L1 holds
+  under an independent FP64 re-evaluation of both marginals (exp included).
+* Both flags leave costs other than the squared one bit-identical to the
+  default form (p = Inf iterates on the squared cost, SinkhornKernel.jl:518-520,
+  so it takes them too).
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dev_inst():
+    import torch
+    from culamp_b200 import datasets as D
+    return tuple(torch.as_tensor(v, device="cuda") for v in D.grid_instance(64, 64, "mixture"))
+
+
+def _np(t):
+    return t.cpu().numpy() if hasattr(t, "cpu") else np.asarray(t)
+
+
+def gauge_free(phi, psi, r):
+    """Sinkhorn's potentials are defined up to (phi + k, psi - k)."""
+    phi, psi = _np(phi), _np(psi)
+    k = np.dot(_np(r), phi) / np.sum(_np(r))
+    return phi - k, psi + k
+
+
+@pytest.mark.parametrize("eta_p", [1e-3, 1e-4])
+def test_fp32_form_follows_fp64_form(dev_inst, eta_p):
+    import culamp_b200 as cb
+    x, y, r, c = dev_inst
+    a = cb.EOTArgs(eta_p=eta_p, epsilon=0.0, itermax=100, verbose=True)
+    ref = cb.solve_sinkhorn(x, y, r, c, a, frequency=10, p=2.0)
+    f32 = cb.solve_sinkhorn(x, y, r, c, a, frequency=10, p=2.0, flags=cb.FLAG_FORM_FP32)
+    assert f32.iterations == ref.iterations and f32.num_iter == ref.num_iter
+    p0, q0 = gauge_free(ref.phi, ref.psi, r)
+    p1, q1 = gauge_free(f32.phi, f32.psi, r)
+    scale = max(1.0, np.abs(p0).max(), np.abs(q0).max())
+    err = max(np.abs(p1 - p0).max(), np.abs(q1 - q0).max()) / scale
+    print(f"eta_p={eta_p}: FP32-form potential error {err:.3e} of max |potential| {scale:.3e}")
+    assert err <= 1e-4
+    assert not np.array_equal(_np(f32.phi), _np(ref.phi))        # the FP32 kernels ran
+    # the FP64 check passes log the same check iterations, residuals close
+    g = np.array([row[1:3] for row in f32.log])
+    w = np.array([row[1:3] for row in ref.log])
+    assert np.array_equal(g[:, 0], w[:, 0])
+    np.testing.assert_allclose(g[:, 1], w[:, 1], rtol=0.2, atol=1e-8)
+
+
+def test_ladder_reaches_tolerance_certified_in_fp64(oracle, dev_inst):
+    import culamp_b200 as cb
+    x, y, r, c = dev_inst
+    kw = dict(eta_p=1e-3, epsilon=6e-6, itermax=20000, verbose=True)
+    ref = cb.solve_sinkhorn(x, y, r, c, cb.EOTArgs(**kw), frequency=10, p=2.0)
+    lad = cb.solve_sinkhorn(x, y, r, c, cb.EOTArgs(**kw), frequency=10, p=2.0, flags=cb.FLAG_LADDER)
+    assert ref.stopped == 1 and lad.stopped == 1
+    assert lad.residual <= 1e-6
+    rl, cl = cb.marginal_error_fp64(x, y, r, c, lad.phi, lad.psi, 1e-3, lad.winf, 2.0)
+    print(f"ladder: {lad.iterations} iterations ({ref.iterations} FP64), {lad.elapsed_ms:.2f} ms "
+          f"({ref.elapsed_ms:.2f} ms FP64), FP64 marginal L1 {rl:.3e} / {cl:.3e}")
+    assert rl <= 1e-6 and cl <= 1e-6
+    # the iteration count stays within a few checks of the FP64 form's
+    assert abs(lad.iterations - ref.iterations) <= 0.1 * ref.iterations + 20
+    # both stop at the same fixed point to the solve's own accuracy
+    p0, q0 = gauge_free(ref.phi, ref.psi, r)
+    p1, q1 = gauge_free(lad.phi, lad.psi, r)
+    scale = max(1.0, np.abs(p0).max())
+    assert np.abs(p1 - p0).max() <= 1e-5 * scale
+    assert np.abs(q1 - q0).max() <= 1e-5 * scale
+    # every logged residual is an FP64 check value and decreases to the stop
+    res = [row[2] for row in lad.log]
+    assert res[-1] == pytest.approx(lad.residual, rel=1e-12)
+
+
+@pytest.mark.parametrize("p", [1.0, 3.0])
+@pytest.mark.parametrize("flag", ["FLAG_FORM_FP32", "FLAG_LADDER"])
+def test_flags_leave_other_costs_unchanged(dev_inst, p, flag):
+    import culamp_b200 as cb
+    x, y, r, c = dev_inst
+    a = cb.EOTArgs(eta_p=1e-3, epsilon=0.0, itermax=30, verbose=True)
+    ref = cb.solve_sinkhorn(x, y, r, c, a, frequency=10, p=p)
+    got = cb.solve_sinkhorn(x, y, r, c, a, frequency=10, p=p, flags=getattr(cb, flag))
+    assert np.array_equal(_np(got.phi), _np(ref.phi))
+    assert np.array_equal(_np(got.psi), _np(ref.psi))
+    assert got.iterations == ref.iterations and got.residual == ref.residual
+
+
+def test_ladder_without_a_tolerance_switches_on_stall(dev_inst):
+    """epsilon = 0 never reaches the switch threshold: the stall rule moves the
+    ladder to FP64 once the FP32 iteration stops gaining, and the residuals of
+    the late checks match the FP64 form's (a ladder stuck in FP32 would show
+    its floor instead)."""
+    import culamp_b200 as cb
+    x, y, r, c = dev_inst
+    a = cb.EOTArgs(eta_p=1e-3, epsilon=0.0, itermax=2500, verbose=True)
+    ref = cb.solve_sinkhorn(x, y, r, c, a, frequency=10, p=2.0)
+    lad = cb.solve_sinkhorn(x, y, r, c, a, frequency=10, p=2.0, flags=cb.FLAG_LADDER)
+    f32 = cb.solve_sinkhorn(x, y, r, c, a, frequency=10, p=2.0, flags=cb.FLAG_FORM_FP32)
+    print(f"2500 iterations: residual FP64 {ref.residual:.3e}, ladder {lad.residual:.3e}, "
+          f"FP32 {f32.residual:.3e}")
+    assert lad.residual <= 2.0 * ref.residual + 1e-12
