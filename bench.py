@@ -66,6 +66,8 @@ def parse():
                          "converged potentials, for profiler captures of the steady-state "
                          "kernel; the potentials are solved for and cached in CACHE.npz "
                          "when it does not exist")
+    ap.add_argument("--profile-form", default="fp64", choices=["fp64", "fp32"],
+                    help="exponent form of the --profile-pass solve")
     ap.add_argument("--profile-feature", type=int, default=0, metavar="N",
                     help="only run warmup + steps Sinkhorn iterations on an N-point d=256 "
                          "feature instance (tensor-core path, pass by pass), for profiler captures")
@@ -129,7 +131,8 @@ def profile_pass(args):
     is a separate kernel launch a profiler can capture). pair_pass_kernel
     launch k (0-based): 0 = W_inf, then 3 per iteration (row LSE, column LSE,
     gated residual), so `-k regex:pair_pass_kernel -s 10 -c 1` captures the
-    row pass of iteration 4 (fixed-reference path)."""
+    row pass of iteration 4 (fixed-reference path). --profile-form picks the
+    FP64-exponent (default) or FP32-exponent passes for the whole solve."""
     import torch
     import culamp_b200 as cb
     from culamp_b200 import datasets as D
@@ -137,9 +140,10 @@ def profile_pass(args):
     x, y, r, c = D.rgb_instance(n, n)
     X, Y, R, Cc = (torch.as_tensor(v, device="cuda") for v in (x, y, r, c))
     a = cb.EOTArgs(eta_p=ETA, epsilon=0.0, itermax=args.warmup + args.steps, verbose=False)
-    res = cb.solve_sinkhorn(X, Y, R, Cc, a, 10**6, P, flags=cb.FLAG_NO_GRAPH)
+    form = cb.FLAG_FORM_FP32 if args.profile_form == "fp32" else cb.FLAG_FORM_FP64
+    res = cb.solve_sinkhorn(X, Y, R, Cc, a, 10**6, P, flags=cb.FLAG_NO_GRAPH | form)
     torch.cuda.synchronize()
-    print(json.dumps({"profile_pass": n, "iterations": res.iterations,
+    print(json.dumps({"profile_pass": n, "form": args.profile_form, "iterations": res.iterations,
                       "finite": bool(torch.isfinite(res.phi).all())}))
     return 0
 
@@ -289,19 +293,19 @@ def reference_arm(args):
     return 0
 
 
-def time_pass(torch, K, stream, X, Y, R, pot, out, winf, reps=50):
+def time_pass(torch, K, stream, X, Y, R, pot, out, winf, reps=50, flags=0):
     """Device time of one in-place row-LSE pass: `reps` launches captured in a
     CUDA graph, replayed and timed with CUDA events on the launching stream
     (falls back to timing host-launched passes if capture is unavailable)."""
     for _ in range(3):
-        K.warp_logsumexp_ct_fused(X, Y, R, pot, ETA, winf, P, out=out)
+        K.warp_logsumexp_ct_fused(X, Y, R, pot, ETA, winf, P, out=out, flags=flags)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     try:
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
             for _ in range(reps):
-                K.warp_logsumexp_ct_fused(X, Y, R, pot, ETA, winf, P, out=out)
+                K.warp_logsumexp_ct_fused(X, Y, R, pot, ETA, winf, P, out=out, flags=flags)
         g.replay()
         torch.cuda.synchronize()
         e0.record()
@@ -313,7 +317,7 @@ def time_pass(torch, K, stream, X, Y, R, pot, out, winf, reps=50):
         torch.cuda.synchronize()
         e0.record(stream)
         for _ in range(reps):
-            K.warp_logsumexp_ct_fused(X, Y, R, pot, ETA, winf, P, out=out)
+            K.warp_logsumexp_ct_fused(X, Y, R, pot, ETA, winf, P, out=out, flags=flags)
         e1.record(stream)
         e1.synchronize()
         return e0.elapsed_time(e1) / reps, f"host-launched ({type(ex).__name__})"
@@ -540,12 +544,17 @@ def extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_chosen, chosen_ms):
     phi5 = s5.phi.clone()
     ms5, how5 = time_pass(torch, K, torch.cuda.current_stream(), X5, Y5, R5, psi5, phi5, s5.winf,
                           reps=10)
+    ms5f, _ = time_pass(torch, K, torch.cuda.current_stream(), X5, Y5, R5, psi5, phi5, s5.winf,
+                        reps=10, flags=cb.FLAG_FORM_FP32)
     ex["sinkhorn_65536"] = {"reached_tol": s5.stopped == 1, "ms": s5.elapsed_ms,
+                            "form": "FP32 -> FP64 ladder (the default at >= 16384^2 pairs)",
+                            "fp32_pass_ms": ms5f, "fp32_pass_gpair_s": 65536.0 ** 2 / (ms5f * 1e-3) / 1e9,
                             "iterations": s5.iterations, "fp64_row_l1": rl, "fp64_col_l1": cl,
                             "pass_ms": ms5, "pass_timing": how5,
                             "pass_gpair_s": 65536.0 ** 2 / (ms5 * 1e-3) / 1e9}
     # the same engine with FP32 exponents, and the FP32 -> FP64 ladder
-    for name, fl in (("fp32_form", cb.FLAG_FORM_FP32), ("ladder", cb.FLAG_LADDER)):
+    # (the default at this size is the FP32 -> FP64 ladder; the other two forms)
+    for name, fl in (("fp32_form", cb.FLAG_FORM_FP32), ("fp64_form", cb.FLAG_FORM_FP64)):
         ex[f"sinkhorn_65536_{name}"] = form_leg(cb, X5, Y5, R5, C5, 25, fl, s5)
     # the plain FP32 form on the same 65536-point instance (capped: it is not
     # expected to reach 1e-6), and LAMP to 1e-6 (marginal test every 25 iterations)

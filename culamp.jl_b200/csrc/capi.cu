@@ -308,6 +308,32 @@ extern "C" int culamp_lse_rows_sk(culamp_handle h, double *out, const double *x,
     return run_pass(h, P, pmode_of(p), ACC_LSE, (cudaStream_t)stream);
 }
 
+extern "C" int culamp_lse_rows_sk_form(culamp_handle h, double *out, const double *x, const double *y,
+                                       int64_t n, int64_t m, int32_t d, const double *marg,
+                                       const double *pot, double reg, double winf, double p,
+                                       uint32_t flags, void *stream) {
+    if (!(flags & CULAMP_FLAG_FORM_FP32))
+        return culamp_lse_rows_sk(h, out, x, y, n, m, d, marg, pot, reg, winf, p, stream);
+    int s = check_common(h, x, y, n, m, d, p);
+    if (s) return s;
+    if (!out || !marg || !pot) return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "null pointer");
+    if (pmode_of(p) != P_SQ || d > MAXD_PACKED)
+        return culamp_set_error(h, CULAMP_ERR_UNSUPPORTED,
+                                "the FP32-exponent form needs p = 2 and d <= %d (got p = %g, d = %d)",
+                                MAXD_PACKED, p, (int)d);
+    PassParams P = base_params(x, y, (int)n, (int)m, d, p);
+    P.ctr = x;
+    P.epi = EPI_SK_ROW;
+    P.alpha = -1.0 / (reg * winf);
+    P.beta = 1.0;
+    P.colpot = pot;
+    P.marg = marg;
+    P.out = out;
+    P.use_ref = 1;
+    P.fp32 = 1;
+    return run_pass(h, P, P_SQ, ACC_LSE, (cudaStream_t)stream);
+}
+
 extern "C" int culamp_residual_sk(culamp_handle h, double *res, double *cost, const double *x,
                                   const double *y, int64_t n, int64_t m, int32_t d,
                                   const double *marg, const double *phi, const double *psi,

@@ -435,6 +435,12 @@ struct SkPlan {
     LaunchShape s_rows, s_cols, s_rows_mom;
 };
 
+// Sinkhorn solves of at least this many pairs take the precision ladder unless
+// CULAMP_FLAG_FORM_FP64 is set. Below it the passes are latency-bound and the
+// FP32-exponent passes save nothing: at 4096^2 the ladder took 86.7 ms against
+// 83.9 ms in FP64, at 65536^2 2.87 s against 4.11 s (same 1e-6 FP64 check).
+constexpr double LADDER_AUTO_PAIRS = 268435456.0;   // 16384^2
+
 // The FP32-exponent forms (FORM_FP32, LADDER) exist for the packed p = 2 passes.
 bool fp32_form_applies(const Solver &S, int d, int pm_iter) {
     return pm_iter == P_SQ && d <= MAXD_PACKED && !S.feat_active;
@@ -490,7 +496,8 @@ SkPlan make_sk_plan(culamp_handle h, int n, int m, int d, double p, uint32_t fla
         if (flags & CULAMP_FLAG_FORM_FP32) {
             pl.k1.fp32 = 1;
             pl.k2.fp32 = 1;
-        } else if (flags & CULAMP_FLAG_LADDER) {
+        } else if ((flags & CULAMP_FLAG_LADDER) ||
+                   (!(flags & CULAMP_FLAG_FORM_FP64) && (double)n * (double)m >= LADDER_AUTO_PAIRS)) {
             // FP32-exponent passes while ctl->fp32_phase holds, FP64 ones after
             pl.ladder = true;
             pl.k1f = pl.k1;

@@ -31,6 +31,7 @@ FLAG_FEAT_X6 = 32
 FLAG_FEAT_FP64 = 64
 FLAG_FORM_FP32 = 128
 FLAG_LADDER = 256
+FLAG_FORM_FP64 = 512
 
 
 class CulampError(RuntimeError):
@@ -96,6 +97,8 @@ SIGNATURES = {
     "culamp_args_from_json_string": (C.c_int, [C.c_char_p, C.POINTER(CArgs)]),
     "culamp_max_cost": (C.c_int, [_VP, _VP, _VP, _I64, _I64, _I32, _D, _VP, C.POINTER(_D), _VP]),
     "culamp_lse_rows_sk": (C.c_int, [_VP, _VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, _D, _D, _D, _VP]),
+    "culamp_lse_rows_sk_form": (C.c_int, [_VP, _VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, _D, _D, _D,
+                                          C.c_uint32, _VP]),
     "culamp_residual_sk": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, _VP,
                                      _D, _D, _D, _VP]),
     "culamp_lse_rows_spp": (C.c_int, [_VP, _VP, _VP, _VP, _I64, _I64, _I32, _VP, _D, _D, _D, _D, _VP]),

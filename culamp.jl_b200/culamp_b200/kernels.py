@@ -36,14 +36,21 @@ def max_logsumexp_spp_ct(x, y, p, rows: bool = True):
     return out, w.value
 
 
-def warp_logsumexp_ct_fused(x, y, marginal, pot, reg, winf, p, out=None):
+def warp_logsumexp_ct_fused(x, y, marginal, pot, reg, winf, p, out=None, flags=0):
     """SinkhornKernel.jl:341-444: log(marg_i) - LSE_j(-C_ij/(reg W) + pot_j).
     With `out` given the result overwrites it in place, and its previous
-    content (the last phi of an iteration) serves as the kernel's reference."""
+    content (the last phi of an iteration) serves as the kernel's reference.
+    flags = FLAG_FORM_FP32 runs the FP32-exponent pass (p = 2, d <= 3)."""
     n, d = x.shape
     m = y.shape[0]
     out = _empty(n, x) if out is None else out
     h = _h(x)
+    if flags:
+        h.check(h._lib.culamp_lse_rows_sk_form(h.ptr, C.c_void_p(out.data_ptr()), _dev(x, "x"),
+                                               _dev(y, "y"), n, m, d, _dev(marginal, "marginal", n),
+                                               _dev(pot, "pot", m), float(reg), float(winf), float(p),
+                                               int(flags), _stream()), "culamp_lse_rows_sk_form")
+        return out
     h.check(h._lib.culamp_lse_rows_sk(h.ptr, C.c_void_p(out.data_ptr()), _dev(x, "x"),
                                       _dev(y, "y"), n, m, d, _dev(marginal, "marginal", n),
                                       _dev(pot, "pot", m), float(reg), float(winf), float(p),

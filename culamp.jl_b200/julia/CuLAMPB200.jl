@@ -24,6 +24,9 @@ const CULAMP_FLAG_FORM_PLAIN = UInt32(8)
 const CULAMP_FLAG_NO_GRAPH = UInt32(16)
 const CULAMP_FLAG_FEAT_X6 = UInt32(32)
 const CULAMP_FLAG_FEAT_FP64 = UInt32(64)
+const CULAMP_FLAG_FORM_FP32 = UInt32(128)
+const CULAMP_FLAG_LADDER = UInt32(256)
+const CULAMP_FLAG_FORM_FP64 = UInt32(512)
 
 # struct culamp_args (EOTArgs, src/Utilities.jl:18-31)
 struct CArgs

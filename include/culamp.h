@@ -62,6 +62,10 @@ extern "C" {
                                           stops falling (not below the previous check's),
                                           then the FP64-exponent form to the tolerance. The
                                           check passes are FP64 in every form.              */
+#define CULAMP_FLAG_FORM_FP64    512u  /* Sinkhorn: FP64-exponent passes throughout. Without it
+                                          (and without FORM_FP32) solves of n m >= 16384^2
+                                          pairs with p = 2 (or the p = Inf quirk) and d <= 3
+                                          take the precision ladder.                        */
 #define CULAMP_FLAG_FEAT_FP64     64u  /* feature clouds on the FP64 pair loops instead of
                                           the tensor cores (exact inner products, slow)     */
 
@@ -132,6 +136,14 @@ int culamp_max_cost(culamp_handle h, const double *x, const double *y, int64_t n
 int culamp_lse_rows_sk(culamp_handle h, double *out, const double *x, const double *y,
                        int64_t n, int64_t m, int32_t d, const double *marg, const double *pot,
                        double reg, double winf, double p, void *stream);
+
+/* culamp_lse_rows_sk with a form: flags = CULAMP_FLAG_FORM_FP32 runs the
+ * FP32-exponent pass (p = 2, d <= 3; CULAMP_ERR_UNSUPPORTED otherwise), 0 the
+ * default pass. The pass the precision ladder runs first; no reference
+ * counterpart (the reference kernel forms its exponents in FP32 throughout). */
+int culamp_lse_rows_sk_form(culamp_handle h, double *out, const double *x, const double *y,
+                            int64_t n, int64_t m, int32_t d, const double *marg, const double *pot,
+                            double reg, double winf, double p, uint32_t flags, void *stream);
 
 /* residual_opt! (SinkhornKernel.jl:9-81): res[i] = marg[i] - sum_j P_ij,
  * cost[i] = sum_j P_ij C_ij with P_ij = exp(-C_ij/(reg*winf) + phi[i] + psi[j]).

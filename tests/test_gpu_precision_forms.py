@@ -114,3 +114,65 @@ def test_ladder_without_a_tolerance_switches_on_stall(dev_inst):
     print(f"2500 iterations: residual FP64 {ref.residual:.3e}, ladder {lad.residual:.3e}, "
           f"FP32 {f32.residual:.3e}")
     assert lad.residual <= 2.0 * ref.residual + 1e-12
+
+
+def test_fp32_pass_against_fp64_pass():
+    """culamp_lse_rows_sk_form (FP32 exponents) against culamp_lse_rows_sk on a
+    20000 x 18000 RGB instance after a few Sinkhorn iterations: the FP32 pass's
+    error is the exponent rounding, a few 2^-24 of the largest exponent term
+    (|alpha C| + |psi| ~ 3e3 here), so <= 1e-3 absolute in log units."""
+    import torch
+    import culamp_b200 as cb
+    from culamp_b200 import datasets as D, kernels as K
+    x, y, r, c = (torch.as_tensor(v, device="cuda") for v in D.rgb_instance(20000, 18000))
+    s = cb.solve_sinkhorn(x, y, r, c, cb.EOTArgs(eta_p=1e-3, epsilon=0.0, itermax=20, verbose=False),
+                          frequency=10, p=2.0)
+    want = s.phi.clone()
+    K.warp_logsumexp_ct_fused(x, y, r, s.psi, 1e-3, s.winf, 2.0, out=want)
+    got = s.phi.clone()
+    K.warp_logsumexp_ct_fused(x, y, r, s.psi, 1e-3, s.winf, 2.0, out=got, flags=cb.FLAG_FORM_FP32)
+    err = (got - want).abs().max().item()
+    print(f"FP32 pass: max |error| {err:.3e} (|phi| <= {want.abs().max().item():.3e})")
+    assert err <= 1e-3
+    assert err > 0.0                                        # the FP32 kernel ran
+    # a stale hint (zeros) takes the FP64 fallbacks and gives the same result
+    cold = torch.zeros_like(want)
+    K.warp_logsumexp_ct_fused(x, y, r, s.psi, 1e-3, s.winf, 2.0, out=cold, flags=cb.FLAG_FORM_FP32)
+    assert (cold - want).abs().max().item() <= 1e-3
+
+
+def test_fp32_pass_rejects_other_costs():
+    import torch
+    import culamp_b200 as cb
+    from culamp_b200 import kernels as K
+    x = torch.rand(64, 3, dtype=torch.float64, device="cuda")
+    r = torch.full((64,), 1 / 64, dtype=torch.float64, device="cuda")
+    out = torch.zeros(64, dtype=torch.float64, device="cuda")
+    with pytest.raises(cb.CulampError):
+        K.warp_logsumexp_ct_fused(x, x, r, torch.zeros_like(r), 1e-2, 1.0, 1.0, out=out,
+                                  flags=cb.FLAG_FORM_FP32)
+    x5 = torch.rand(64, 5, dtype=torch.float64, device="cuda")
+    with pytest.raises(cb.CulampError):
+        K.warp_logsumexp_ct_fused(x5, x5, r, torch.zeros_like(r), 1e-2, 1.0, 2.0, out=out,
+                                  flags=cb.FLAG_FORM_FP32)
+
+
+def test_default_form_takes_the_ladder_above_16384_squared():
+    """At n m >= 16384^2 the default is the ladder: same result as
+    FLAG_LADDER bit for bit, and FLAG_FORM_FP64 gives the FP64 form; both
+    certified to 1e-6 by the FP64 re-check."""
+    import torch
+    import culamp_b200 as cb
+    from culamp_b200 import datasets as D
+    x, y, r, c = (torch.as_tensor(v, device="cuda") for v in D.rgb_instance(16384, 16384))
+    a = cb.EOTArgs(eta_p=1e-3, epsilon=6e-6, itermax=5000, verbose=False)
+    dflt = cb.solve_sinkhorn(x, y, r, c, a, frequency=25, p=2.0)
+    lad = cb.solve_sinkhorn(x, y, r, c, a, frequency=25, p=2.0, flags=cb.FLAG_LADDER)
+    f64 = cb.solve_sinkhorn(x, y, r, c, a, frequency=25, p=2.0, flags=cb.FLAG_FORM_FP64)
+    print(f"16384: default {dflt.iterations} it {dflt.elapsed_ms:.1f} ms, FP64 form "
+          f"{f64.iterations} it {f64.elapsed_ms:.1f} ms")
+    assert torch.equal(dflt.phi, lad.phi) and dflt.iterations == lad.iterations
+    for res in (dflt, f64):
+        assert res.stopped == 1
+        rl, cl = cb.marginal_error_fp64(x, y, r, c, res.phi, res.psi, 1e-3, res.winf, 2.0)
+        assert rl <= 1e-6 and cl <= 1e-6
