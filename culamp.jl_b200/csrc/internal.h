@@ -145,6 +145,18 @@ cudaError_t launch_pass_batched(const PassParams *plist, const int *block_start,
                                 int total_blocks, size_t smem, int pmode, int d, int acc, bool mom,
                                 bool fixed_ref, cudaStream_t st);
 
+// ---- whole Sinkhorn loop in one persistent cooperative launch (persist.cu):
+// small problems (p = 1, 2 or Inf with the same cost in the check, d <= 3).
+bool persist_eligible(int n, int m, int d, int pm_iter, int pm_resid);
+int persist_grid(int sm_count, int d, int pm);          // CTAs (0: not launchable)
+size_t persist_scratch_bytes(int grid);
+// The loop from the control block's state to its stop; `scratch` holds
+// persist_scratch_bytes(grid) bytes. Completes the control block like the
+// pass-per-launch loop (iteration counters, stop reason, residual, log).
+cudaError_t launch_sk_persist(const double *X, const double *Y, const double *r, const double *c,
+                              double *phi, double *psi, int n, int m, int d, int pm, double pexp,
+                              Ctl *ctl, void *scratch, int grid, cudaStream_t st);
+
 }  // namespace culamp_host
 
 // The opaque handle.

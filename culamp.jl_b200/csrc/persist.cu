@@ -1,0 +1,585 @@
+// persist.cu -- the whole Sinkhorn loop of a small problem in one persistent
+// launch (SinkhornKernel.jl:477-559 with the passes of :341-444 and :9-81).
+//
+// At n, m of a few thousand points a pass is ~10 microseconds of pair work
+// spread over 148 SMs, and a pass-per-launch loop pays for each pass a launch,
+// a prologue that stages the rows, and a merge of column-split partials by the
+// last CTA of each row block (a dependent round trip through L2). Here one
+// cooperative launch of one CTA per SM runs every iteration:
+//
+//   * CTA b owns the output rows [b n / G, (b+1) n / G) of each half-step (G =
+//     grid size), so a row's log-sum-exp is finished inside its CTA: no split
+//     partials, no tickets. Its 16 warps spread the columns over their lanes,
+//     four columns per thread in registers, and walk the CTA's rows (14 at a
+//     time, their data broadcast from shared memory). The per-thread column
+//     sums are merged across each warp by a butterfly reduce-scatter and across
+//     the warps in shared memory in a fixed order.
+//   * Each term uses the fixed-reference exponent of the pass engine (DADD with
+//     FR_MAGIC, funnel-shifted mantissa, one MUFU ex2, exponent-field add,
+//     scaled by 2^FR_C0). A row whose sum leaves the window is recomputed by one
+//     warp with an FP64 online log-sum-exp (exact exp) over all columns.
+//   * Half-steps are separated by a grid barrier (one arrival counter and one
+//     generation word in global memory). Every wait on it is bounded: after
+//     PERSIST_WAIT_NS a waiting CTA sets the abort word and the control block's
+//     error flag and every CTA leaves the loop; the host reports a device
+//     timeout.
+//   * The control step of each iteration (iteration counter, check cadence,
+//     itermax, tmax, the tolerance test of the check iterations) follows the
+//     pass engine's FIN_SK_ITER / FIN_SK_CHECK. Decisions that every CTA needs
+//     are computed by every CTA from the same data in the same order (the
+//     tolerance test sums the per-CTA partials in CTA order); the one decision
+//     that reads the clock (tmax) is taken by CTA 0 and published before it
+//     arrives at the barrier. CTA 0 alone writes the control block and the log.
+//
+// Potentials written by other CTAs are read with L2-coherent loads (ld.cg).
+
+#include "internal.h"
+
+namespace culamp_dev {
+
+constexpr int PTPB = 512;                  // threads per CTA (one CTA per SM)
+constexpr int PWARPS = PTPB / 32;
+constexpr int PRG = 14;                    // rows per group
+constexpr unsigned long long PERSIST_WAIT_NS = 2000000000ull;
+constexpr int PERSIST_MAX_POINTS = 16384;  // per side: <= 16 terms per thread partial
+constexpr double PERSIST_MAX_PAIRS = 134217728.0;   // 2^27 pairs (8192 x 16384)
+
+struct GridBar {
+    unsigned count;    // arrivals at the current barrier
+    unsigned gen;      // completed barriers
+    unsigned abort;    // set by a CTA that gave up waiting
+    unsigned tmax_hit; // CTA 0's clock decision for the current iteration
+};
+
+struct PersistParams {
+    const double *X, *Y;       // point clouds (n x d, m x d), read-only
+    const double *r, *c;       // marginals
+    double *phi, *psi;         // potentials, updated in place
+    int n, m;
+    double pexp;
+    Ctl *ctl;
+    double *blk;               // [G][4] per-CTA partial sums (fixed-order totals)
+    GridBar *bar;              // zeroed before the launch
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier with a bounded wait. Returns false (in every thread of the
+// CTA) when this CTA gave up or saw another CTA give up.
+__device__ bool grid_sync(GridBar *gb, unsigned &gen, int *s_flag) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        __threadfence();
+        const unsigned g = gen;
+        if (atomicAdd(&gb->count, 1u) == gridDim.x - 1u) {
+            atomicExch(&gb->count, 0u);
+            __threadfence();
+            atomicExch(&gb->gen, g + 1u);
+        } else {
+            const unsigned long long t0 = globaltimer_ns();
+            unsigned spins = 0;
+            while (ld_acquire_u32(&gb->gen) == g) {
+                if (ld_acquire_u32(&gb->abort)) { ok = 0; break; }
+                if (++spins > 64u) {
+                    if (globaltimer_ns() - t0 > PERSIST_WAIT_NS) {
+                        atomicExch(&gb->abort, 1u);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+        }
+        __threadfence();
+        *s_flag = ok;
+    }
+    gen += 1u;
+    __syncthreads();
+    return *s_flag != 0;
+}
+
+// One half-step's geometry and coefficients. Rows: the points whose potential
+// is written (X side), columns: the others.
+struct Half {
+    const double *Xr, *Yc;     // row points, column points
+    const double *marg;        // row marginal
+    const double *colpot;      // column potential (read through L2)
+    double *rowpot;            // row potential: reference in, result out
+    int nr, nc;
+};
+
+struct PShared {
+    double4 row[PRG];          // p = 2: {-2 a2 v, K}; else {v, K} (v = x - ctr)
+    float4 rowf[PRG];          // v in FP32 (p = 2 cost moment)
+    double hm[PRG][2];         // H (a2 |v|^2 for p = 2, else 0), M2 = reference - H (log2 units)
+    float red[PWARPS][16];
+    float redm[PWARPS][16];
+    double L[PRG], E[PRG];     // natural-log LSE, softmax-weighted mean cost
+    int bad[PRG];
+    double con[PRG][3];        // per-row contributions to the CTA's partial sums
+    int flag;
+};
+
+// Butterfly reduce-scatter of 16 values over a warp: afterwards lane l holds in
+// a[0] the warp total of value l >> 1 (16 shuffles instead of 16 x 5).
+__device__ __forceinline__ void warp_scatter16(float (&a)[16]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 16, L = 16; o >= 2; o >>= 1, L >>= 1) {
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int i = 0; i < L / 2; ++i) {
+            const float send = up ? a[i] : a[i + L / 2];
+            const float keep = up ? a[i + L / 2] : a[i];
+            a[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    a[0] += __shfl_xor_sync(0xffffffffu, a[0], 1);
+}
+
+// One fixed-reference term from dv = t - Mref - 1 + FR_MAGIC (see the pass
+// engine's tile_lse_fixedref): 2^(t - Mref) * 2^C0 for t - Mref in
+// [-C0, 126 - C0]. ZLOW: a term below the window becomes a subnormal (< 2^-126)
+// instead of ~2..4, so it adds nothing to a moment -- the check pass's cost
+// moment keeps terms down to 2^-C0 of the reference and no floor below them.
+template <int C0, bool ZLOW>
+__device__ __forceinline__ float fr_term(double dv) {
+    const int hi = __double2hiint(dv);
+    const float vm = __int_as_float((int)__funnelshift_r((unsigned)__double2loint(dv), 0x7Fu, 9));
+    const int eb = __float_as_int(ex2_approx(vm));
+    int k;
+    if constexpr (!ZLOW) {
+        asm("{.reg .s32 t;\n\tadd.s32 t, %1, %2;\n\tmin.s32.relu %0, t, %3;}"
+            : "=r"(k) : "r"(hi), "n"(C0 - FR_H0), "n"(126));
+        return __int_as_float(eb + (k << 23));
+    } else {
+        asm("{.reg .s32 t;\n\tadd.s32 t, %1, %2;\n\tmin.s32.relu %0, t, %3;}"
+            : "=r"(k) : "r"(hi), "n"(C0 + 128 - FR_H0), "n"(254));
+        return __int_as_float(eb + (k << 23) - (128 << 23));
+    }
+}
+
+// Exact FP64 online log-sum-exp of one row over all columns, by one warp:
+// the recompute of a row whose fixed-reference sum left the window.
+template <int PM, int D>
+__device__ void row_lse_exact(const Half &H, int o, double alpha, double inv_winf, double pexp,
+                              double &L, double &Ec) {
+    const int lane = threadIdx.x & 31;
+    double xv[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) xv[k] = H.Xr[(size_t)o * D + k];
+    double M = -INFINITY, S = 0.0, MO = 0.0;
+    for (int j = lane; j < H.nc; j += 32) {
+        double yv[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) yv[k] = H.Yc[(size_t)j * D + k];
+        const double cc = pair_cost_direct<PM>(xv, yv, D, pexp);
+        const double t = fma(alpha, cc, __ldcg(H.colpot + j));
+        const double cn = cc * inv_winf;
+        if (t == -INFINITY) continue;
+        if (t > M) {
+            const double f = exp(M - t);
+            S = S * f + 1.0;
+            MO = MO * f + cn;
+            M = t;
+        } else {
+            const double e = exp(t - M);
+            S += e;
+            MO = fma(e, cn, MO);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const double M2 = __shfl_xor_sync(0xffffffffu, M, off);
+        const double S2 = __shfl_xor_sync(0xffffffffu, S, off);
+        const double MO2 = __shfl_xor_sync(0xffffffffu, MO, off);
+        if (M2 == -INFINITY) continue;
+        if (M == -INFINITY) { M = M2; S = S2; MO = MO2; continue; }
+        if (M2 > M) {
+            const double f = exp(M - M2);
+            S = S * f + S2;
+            MO = MO * f + MO2;
+            M = M2;
+        } else {
+            const double f = exp(M2 - M);
+            S += S2 * f;
+            MO += MO2 * f;
+        }
+    }
+    L = M + log(S);
+    Ec = (S > 0.0) ? MO / S * (1.0 / inv_winf) : 0.0;
+}
+
+// Log-sum-exp of one group of up to PRG rows [row0, row0 + nrows) against all
+// columns; leaves L (and with MOM the mean cost) of each row in sh.L / sh.E.
+// Reference of row o: log(marg_o) - rowpot_o, its previous log-sum-exp (the
+// row update) or the one the check's potentials were made from (the check).
+template <int PM, int D, bool MOM, int CB>
+__device__ void group_lse(const Half &H, int row0, int nrows, const double (&ctr)[D], double a2,
+                          double inv_winf, double pexp, PShared &sh) {
+    constexpr bool SQ = (PM == P_SQ);
+    // window exponent: the row update's LSE may move well above its reference
+    // (FR_C0 leaves 46 above); the check's hardly moves, and its cost moment
+    // wants the small terms
+    constexpr int C0 = MOM ? 120 : FR_C0;
+    static_assert(CB == 2 || CB == 4, "columns per thread step");
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid < PRG) {
+        const int o = row0 + tid;
+        const bool ok = tid < nrows;
+        double v[3] = {0.0, 0.0, 0.0};
+        double h = 0.0;
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            v[k] = ok ? H.Xr[(size_t)o * D + k] - ctr[k] : 0.0;
+            h = fma(v[k], v[k], h);
+        }
+        const double Hh = SQ ? a2 * h : 0.0;
+        const double ref = ok ? log(H.marg[o]) - __ldcg(H.rowpot + o) : 0.0;
+        const double M2 = ref * LOG2E - Hh;
+        sh.row[tid] = SQ ? make_double4(-2.0 * a2 * v[0], -2.0 * a2 * v[1], -2.0 * a2 * v[2], FR_MAGIC - (M2 + 1.0))
+                         : make_double4(v[0], v[1], v[2], FR_MAGIC - (M2 + 1.0));
+        sh.rowf[tid] = make_float4((float)v[0], (float)v[1], (float)v[2], 0.f);
+        sh.hm[tid][0] = Hh;
+        sh.hm[tid][1] = M2;
+    }
+    __syncthreads();
+    unsigned long long acc[PRG], mo[MOM ? PRG : 1];
+#pragma unroll
+    for (int r = 0; r < PRG; ++r) acc[r] = 0ull;
+#pragma unroll
+    for (int r = 0; r < (MOM ? PRG : 1); ++r) mo[r] = 0ull;
+    const float invw_f = (float)inv_winf;
+    for (int jb = 0; jb < H.nc; jb += CB * PTPB) {
+        double4 col[CB];
+        float cfy[(MOM && SQ) ? CB : 1][3];
+#pragma unroll
+        for (int c = 0; c < CB; ++c) {
+            const int j = jb + c * PTPB + tid;
+            double yy[3] = {0.0, 0.0, 0.0};
+            double g = -INFINITY;
+            if (j < H.nc) {
+                double s2 = 0.0;
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+                    yy[k] = H.Yc[(size_t)j * D + k] - ctr[k];
+                    s2 = fma(yy[k], yy[k], s2);
+                }
+                g = LOG2E * __ldcg(H.colpot + j);
+                if (SQ) g += a2 * s2;
+            }
+            col[c] = make_double4(yy[0], yy[1], yy[2], g);
+            if constexpr (MOM && SQ) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) cfy[c][k] = (float)yy[k];
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < PRG; ++r) {
+            const double4 rd = sh.row[r];
+            float e[CB], cf[CB];
+#pragma unroll
+            for (int c = 0; c < CB; ++c) {
+                double t;
+                cf[c] = 0.f;
+                if (SQ) {
+                    t = col[c].w;
+                    if (D >= 3) t = fma(rd.z, col[c].z, t);
+                    if (D >= 2) t = fma(rd.y, col[c].y, t);
+                    t = fma(rd.x, col[c].x, t);
+                } else {
+                    const double xv[3] = {rd.x, rd.y, rd.z};
+                    const double yv[3] = {col[c].x, col[c].y, col[c].z};
+                    const double cc = pair_cost_direct<PM>(xv, yv, D, pexp);
+                    t = fma(cc, a2, col[c].w);
+                    if (MOM) cf[c] = (float)(cc * inv_winf);
+                }
+                e[c] = fr_term<C0, MOM>(t + rd.w);
+            }
+            if constexpr (MOM && SQ) {
+                const float4 rf = sh.rowf[r];
+#pragma unroll
+                for (int c = 0; c < CB; ++c) {
+                    const float d0 = rf.x - cfy[c][0], d1 = rf.y - cfy[c][1], d2 = rf.z - cfy[c][2];
+                    cf[c] = fmaf(d2, d2, fmaf(d1, d1, d0 * d0)) * invw_f;
+                }
+            }
+            acc[r] = add_f32x2(acc[r], pack_f32x2(e[0], e[1]));
+            if (CB == 4) acc[r] = add_f32x2(acc[r], pack_f32x2(e[CB == 4 ? 2 : 0], e[CB == 4 ? 3 : 1]));
+            if constexpr (MOM) {
+                mo[r] = fma_f32x2(pack_f32x2(e[0], e[1]), pack_f32x2(cf[0], cf[1]), mo[r]);
+                if (CB == 4)
+                    mo[r] = fma_f32x2(pack_f32x2(e[CB == 4 ? 2 : 0], e[CB == 4 ? 3 : 1]),
+                                      pack_f32x2(cf[CB == 4 ? 2 : 0], cf[CB == 4 ? 3 : 1]), mo[r]);
+            }
+        }
+    }
+    {
+        float a[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) a[r] = (r < PRG) ? lo_f32(acc[r < PRG ? r : 0]) + hi_f32(acc[r < PRG ? r : 0]) : 0.f;
+        warp_scatter16(a);
+        if ((lane & 1) == 0 && (lane >> 1) < PRG) sh.red[warp][lane >> 1] = a[0];
+    }
+    if constexpr (MOM) {
+        float a[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) a[r] = (r < PRG) ? lo_f32(mo[r < PRG ? r : 0]) + hi_f32(mo[r < PRG ? r : 0]) : 0.f;
+        warp_scatter16(a);
+        if ((lane & 1) == 0 && (lane >> 1) < PRG) sh.redm[warp][lane >> 1] = a[0];
+    }
+    __syncthreads();
+    if (tid < nrows) {
+        double S = 0.0, MOv = 0.0;
+#pragma unroll
+        for (int w = 0; w < PWARPS; ++w) {
+            S += (double)sh.red[w][tid];
+            if (MOM) MOv += (double)sh.redm[w][tid];
+        }
+        // the window: no term clamped high (S <= 2^126 scaled), and the full
+        // sum within C0 - 32 - log2(nc) below the reference (the engine's
+        // fr_low_margin), i.e. log2(S) >= 32 + log2(nc)
+        const bool good = S > 0.0 && S <= FR_SUM_MAX && log2(S) >= 32.0 + log2((double)H.nc);
+        sh.bad[tid] = !good;
+        if (good) {
+            sh.L[tid] = LN2 * (sh.hm[tid][0] + sh.hm[tid][1] + (log2(S) - (double)C0));
+            sh.E[tid] = MOM ? MOv / S / inv_winf : 0.0;
+        }
+    }
+    __syncthreads();
+    for (int rr = warp; rr < nrows; rr += PWARPS) {
+        if (!sh.bad[rr]) continue;
+        double L, Ec;
+        row_lse_exact<PM, D>(H, row0 + rr, a2 * LN2, inv_winf, pexp, L, Ec);
+        if (lane == 0) { sh.L[rr] = L; sh.E[rr] = Ec; }
+    }
+    __syncthreads();
+}
+
+enum HalfMode { HM_ROW = 0, HM_CHECK = 1 };
+
+// One half-step over this CTA's rows. HM_ROW: rowpot = log(marg) - L
+// (EPI_SK_ROW), part[0] = sum marg . rowpot. HM_CHECK: the row residual of
+// residual_opt! (EPI_SK_RESID): part = {sum |marg - mass|, sum mass E[C],
+// sum marg . rowpot}. part is valid in thread 0, summed in row order.
+template <int PM, int D, bool MOM, int CB>
+__device__ void half_step(const Half &H, const double (&ctr)[D], double a2, double inv_winf,
+                          double pexp, int mode, PShared &sh, double (&part)[3]) {
+    const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+    const int r_lo = (int)(((long long)b * H.nr) / G);
+    const int r_hi = (int)(((long long)(b + 1) * H.nr) / G);
+    part[0] = part[1] = part[2] = 0.0;
+    for (int row0 = r_lo; row0 < r_hi; row0 += PRG) {
+        const int nrows = min(PRG, r_hi - row0);
+        group_lse<PM, D, MOM, CB>(H, row0, nrows, ctr, a2, inv_winf, pexp, sh);
+        if (tid < nrows) {
+            const int o = row0 + tid;
+            const double L = sh.L[tid];
+            if (mode == HM_ROW) {
+                const double v = log(H.marg[o]) - L;
+                H.rowpot[o] = v;
+                sh.con[tid][0] = H.marg[o] * v;
+                sh.con[tid][1] = sh.con[tid][2] = 0.0;
+            } else {
+                const double f = __ldcg(H.rowpot + o);
+                const double mass = exp(f + L);
+                sh.con[tid][0] = fabs(H.marg[o] - mass);
+                sh.con[tid][1] = mass * sh.E[tid];
+                sh.con[tid][2] = H.marg[o] * f;
+            }
+        }
+        __syncthreads();
+        if (tid == 0)
+            for (int r = 0; r < nrows; ++r)
+                for (int k = 0; k < 3; ++k) part[k] += sh.con[r][k];
+    }
+}
+
+// Sum over CTAs of slot k of the per-CTA partials, in CTA order (the same
+// value in every CTA). Thread 0 only.
+__device__ __forceinline__ double cta_total(const double *blk, int k) {
+    double s = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(blk + b * 4 + k);
+    return s;
+}
+
+// The Sinkhorn loop (SinkhornKernel.jl:477-559): row update, column update,
+// and every `frequency` iterations the residual check, until the tolerance,
+// itermax or tmax stops it; the control step of each iteration as in
+// FIN_SK_ITER / FIN_SK_CHECK.
+template <int PM, int D>
+__global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_constant__ PersistParams P) {
+    __shared__ PShared sh;
+    __shared__ double s_tot[4];
+    __shared__ int s_stop;
+    Ctl *ctl = P.ctl;
+    if (ctl->stop) return;
+    const double alpha = -1.0 / (ctl->eta * ctl->winf);
+    const double a2 = alpha * LOG2E;
+    const double inv_winf = 1.0 / ctl->winf;
+    double ctr[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) ctr[k] = P.X[k];
+    const Half rowh{P.X, P.Y, P.r, P.psi, P.phi, P.n, P.m};
+    const Half colh{P.Y, P.X, P.c, P.phi, P.psi, P.m, P.n};
+    long long iter = ctl->iter, num_iter = ctl->num_iter;
+    const long long itermax = ctl->itermax, freq = ctl->frequency;
+    const double tol = ctl->epsilon / 6.0;
+    const int b = blockIdx.x, tid = threadIdx.x;
+    unsigned gen = 0;
+    double part[3];
+    int stop_reason = 0;
+    bool checked = false, failed = false;
+    double residual = 0.0, objective = 0.0;
+    for (;;) {
+        half_step<PM, D, false, 4>(rowh, ctr, a2, inv_winf, P.pexp, HM_ROW, sh, part);
+        if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
+        half_step<PM, D, false, 4>(colh, ctr, a2, inv_winf, P.pexp, HM_ROW, sh, part);
+        if (tid == 0) {
+            P.blk[b * 4 + 0] = part[0];
+            if (b == 0) {
+                const bool late = (double)(globaltimer_ns() - ctl->t_start_ns) * 1e-9 > ctl->tmax_s;
+                atomicExch(&P.bar->tmax_hit, late ? 1u : 0u);
+            }
+        }
+        if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
+        // FIN_SK_ITER, the same in every CTA
+        iter += 1;
+        int pending = 0;
+        if (iter >= itermax) pending = 2;
+        else if (ld_acquire_u32(&P.bar->tmax_hit)) pending = 3;
+        const bool do_check = ((iter - 1) % freq) == 0;
+        if (!do_check) {
+            num_iter += 1;
+            if (pending) { stop_reason = pending; break; }
+            continue;
+        }
+        half_step<PM, D, true, 2>(rowh, ctr, a2, inv_winf, P.pexp, HM_CHECK, sh, part);
+        if (tid == 0) {
+            P.blk[b * 4 + 1] = part[0];
+            P.blk[b * 4 + 2] = part[1];
+            P.blk[b * 4 + 3] = part[2];
+        }
+        if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
+        // FIN_SK_CHECK, the same in every CTA
+        if (tid == 0) {
+            for (int k = 0; k < 4; ++k) s_tot[k] = cta_total(P.blk, k);
+            const double l1 = s_tot[1];
+            int st = 0;
+            if (l1 <= tol) st = 1;
+            else if (pending) st = pending;
+            if (b == 0) put_log(ctl, (double)iter, l1, s_tot[2], nan(""), s_tot[0] + s_tot[3]);
+            s_stop = st;
+        }
+        __syncthreads();
+        checked = true;
+        residual = s_tot[1];
+        objective = s_tot[2];
+        if (s_stop != 1) num_iter += 1;
+        if (s_stop) { stop_reason = s_stop; break; }
+    }
+    if (tid != 0) return;
+    if (failed) {
+        ctl->error = 1;
+        ctl->stop = 1;
+        return;
+    }
+    if (b != 0) return;
+    // CTA 0 writes the state the pass-per-launch loop leaves behind
+    ctl->dualval = cta_total(P.blk, 0);
+    ctl->iter = iter;
+    ctl->num_iter = num_iter;
+    ctl->stop = 1;
+    ctl->stop_reason = stop_reason;
+    ctl->pending_stop = (stop_reason >= 2) ? stop_reason : 0;
+    if (checked) {
+        ctl->residual = residual;
+        ctl->objective = objective;
+    }
+}
+
+}  // namespace culamp_dev
+
+namespace culamp_host {
+
+using namespace culamp_dev;
+
+bool persist_eligible(int n, int m, int d, int pm_iter, int pm_resid) {
+    if (pm_iter != pm_resid) return false;
+    if (pm_iter != P_L1 && pm_iter != P_SQ && pm_iter != P_INF) return false;
+    if (d < 1 || d > MAXD_PACKED) return false;
+    // each thread's FP32 partial covers at most 16 terms per packed half
+    if (n > PERSIST_MAX_POINTS || m > PERSIST_MAX_POINTS) return false;
+    return (double)n * (double)m <= PERSIST_MAX_PAIRS;
+}
+
+size_t persist_scratch_bytes(int grid) {
+    return (size_t)grid * 4 * sizeof(double) + sizeof(GridBar);
+}
+
+namespace {
+
+template <int PM>
+cudaError_t launch_pm(int d, const cudaLaunchConfig_t &cfg, const PersistParams &P) {
+    switch (d) {
+        case 1: return cudaLaunchKernelEx(&cfg, sk_persist_kernel<PM, 1>, P);
+        case 2: return cudaLaunchKernelEx(&cfg, sk_persist_kernel<PM, 2>, P);
+        default: return cudaLaunchKernelEx(&cfg, sk_persist_kernel<PM, 3>, P);
+    }
+}
+
+}  // namespace
+
+int persist_grid(int sm_count, int d, int pm) {
+    int per_sm = 0;
+    cudaError_t e;
+    if (pm == P_SQ)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, d == 1 ? sk_persist_kernel<P_SQ, 1> : d == 2 ? sk_persist_kernel<P_SQ, 2> : sk_persist_kernel<P_SQ, 3>,
+            PTPB, 0);
+    else if (pm == P_L1)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, d == 1 ? sk_persist_kernel<P_L1, 1> : d == 2 ? sk_persist_kernel<P_L1, 2> : sk_persist_kernel<P_L1, 3>,
+            PTPB, 0);
+    else
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, d == 1 ? sk_persist_kernel<P_INF, 1> : d == 2 ? sk_persist_kernel<P_INF, 2> : sk_persist_kernel<P_INF, 3>,
+            PTPB, 0);
+    if (e != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        return 0;
+    }
+    return sm_count;   // one CTA per SM
+}
+
+cudaError_t launch_sk_persist(const double *X, const double *Y, const double *r, const double *c,
+                              double *phi, double *psi, int n, int m, int d, int pm, double pexp,
+                              Ctl *ctl, void *scratch, int grid, cudaStream_t st) {
+    PersistParams P;
+    P.X = X; P.Y = Y; P.r = r; P.c = c; P.phi = phi; P.psi = psi;
+    P.n = n; P.m = m; P.pexp = pexp; P.ctl = ctl;
+    P.blk = reinterpret_cast<double *>(scratch);
+    P.bar = reinterpret_cast<GridBar *>(P.blk + (size_t)grid * 4);
+    cudaError_t e = cudaMemsetAsync(P.bar, 0, sizeof(GridBar), st);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(PTPB);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;   // all CTAs co-resident, or the launch fails
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    if (pm == P_SQ) return launch_pm<P_SQ>(d, cfg, P);
+    if (pm == P_L1) return launch_pm<P_L1>(d, cfg, P);
+    return launch_pm<P_INF>(d, cfg, P);
+}
+
+}  // namespace culamp_host

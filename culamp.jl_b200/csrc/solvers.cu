@@ -84,6 +84,7 @@ struct culamp_handle_s::Solver {
     long long generation = 0;
     DevBuf X, Y, r, c, phi, psi, res, cost, logz, aux, nu, nub, theta, thetab, eta_mu, tmp, ctl,
         logbuf, setup, ws_phi, ws_psi, prev_phi, prev_psi;
+    DevBuf pers;               // persistent loop: per-CTA partials + grid barrier
     DevBuf hx, hy;             // host-variant staging (device side)
     // feature-cost path: both clouds as bf16 pieces in the MMA tile image + norms
     DevBuf fx, fy, fxn, fyn;
@@ -106,7 +107,7 @@ struct culamp_handle_s::Solver {
         drop_graphs();
         DevBuf *all[] = {&X, &Y, &r, &c, &phi, &psi, &res, &cost, &logz, &aux, &nu, &nub, &theta,
                          &thetab, &eta_mu, &tmp, &ctl, &logbuf, &setup, &ws_phi, &ws_psi,
-                         &prev_phi, &prev_psi, &hx, &hy, &fx, &fy, &fxn, &fyn};
+                         &prev_phi, &prev_psi, &pers, &hx, &hy, &fx, &fy, &fxn, &fyn};
         for (DevBuf *b : all) b->release();
         scr.release();
         if (cap_stream) cudaStreamDestroy(cap_stream);
@@ -562,8 +563,23 @@ int sinkhorn_loop(culamp_handle h, int n, int m, int d, double p, double eta, do
         body_pos = (body_pos + 1) % unroll;
         return iteration(s, with_check);
     };
+    const bool persist = !(flags & (CULAMP_FLAG_NO_GRAPH | CULAMP_FLAG_NO_PERSIST)) && !pl.ladder &&
+                         !pl.k1.fp32 && !S.feat_active && persist_eligible(n, m, d, pl.pm_iter, pl.pm_resid);
+    const int pgrid = persist ? persist_grid(h->sm_count, d, pl.pm_iter) : 0;
+    if (pgrid > 0) CUDA_TRY(h, S.pers.reserve(persist_scratch_bytes(pgrid)));
     CUDA_TRY(h, cudaEventRecord(S.ev0, st));
-    if (flags & CULAMP_FLAG_NO_GRAPH) {
+    bool ran = false;
+    if (pgrid > 0) {
+        // the whole loop in one cooperative launch; a refused launch (e.g. the
+        // CTAs cannot all be resident) falls back to the graph loop
+        const cudaError_t e = launch_sk_persist(S.X.as<double>(), S.Y.as<double>(), S.r.as<double>(),
+                                                S.c.as<double>(), S.phi.as<double>(), S.psi.as<double>(), n, m,
+                                                d, pl.pm_iter, pl.k1.pexp, S.ctl.as<Ctl>(), S.pers.ptr, pgrid, st);
+        if (e == cudaSuccess) ran = true;
+        else cudaGetLastError();
+    }
+    if (ran) {
+    } else if (flags & CULAMP_FLAG_NO_GRAPH) {
         // host-driven loop: check the stop flag after every iteration
         for (long long it = 0; it < args->itermax + 2; ++it) {
             CUDA_TRY(h, iteration(st, true));

@@ -32,6 +32,7 @@ FLAG_FEAT_FP64 = 64
 FLAG_FORM_FP32 = 128
 FLAG_LADDER = 256
 FLAG_FORM_FP64 = 512
+FLAG_NO_PERSIST = 1024
 
 
 class CulampError(RuntimeError):

@@ -27,6 +27,7 @@ const CULAMP_FLAG_FEAT_FP64 = UInt32(64)
 const CULAMP_FLAG_FORM_FP32 = UInt32(128)
 const CULAMP_FLAG_LADDER = UInt32(256)
 const CULAMP_FLAG_FORM_FP64 = UInt32(512)
+const CULAMP_FLAG_NO_PERSIST = UInt32(1024)
 
 # struct culamp_args (EOTArgs, src/Utilities.jl:18-31)
 struct CArgs

@@ -2,7 +2,8 @@
 
 Every instance of a batch must come out as if solved alone. On the FP64-
 exponent pair path (d <= 3, and other d on the FP64 loops): the same stopping
-iteration as culamp_sinkhorn at a tolerance the residual crosses decisively,
+iteration as culamp_sinkhorn's pass-per-launch loop (CULAMP_FLAG_NO_PERSIST,
+the passes a batch runs) at a tolerance the residual crosses decisively,
 and the same potentials up to summation order (the batch sizes its column
 splits for the batch, not for the instance alone), gauge-fixed within 5e-6.
 At epsilon = 1e-6 the residual decays slowly through the threshold, and the
@@ -46,7 +47,7 @@ def test_batch_matches_single_solves(batch, frequency):
     assert out.target_ctas_per_sm in (2, 4, 8, 16)
     assert len(out.results) == len(dev)
     for k, ((x, y, r, c), res) in enumerate(zip(dev, out.results)):
-        one = cb.solve_sinkhorn(x, y, r, c, a, frequency, 2.0)
+        one = cb.solve_sinkhorn(x, y, r, c, a, frequency, 2.0, flags=cb.FLAG_NO_PERSIST)
         feat = x.shape[1] >= 32
         assert res.stopped == one.stopped == 1, k
         # at 1e-6 the residual crosses the threshold slowly, so rounding that
@@ -75,7 +76,7 @@ def test_batch_stops_at_single_solver_iteration(batch):
     for k, ((x, y, r, c), res) in enumerate(zip(dev, out.results)):
         if x.shape[1] >= 32:
             continue
-        one = cb.solve_sinkhorn(x, y, r, c, a, 5, 2.0)
+        one = cb.solve_sinkhorn(x, y, r, c, a, 5, 2.0, flags=cb.FLAG_NO_PERSIST)
         assert (res.iterations, res.num_iter, res.stopped) == (one.iterations, one.num_iter, 1), k
 
 
@@ -116,7 +117,7 @@ def test_batch_l1_cost_and_graphless_loop(batch):
     g = cb.solve_batched_sinkhorn(small, a, frequency=3, p=1.0)
     h = cb.solve_batched_sinkhorn(small, a, frequency=3, p=1.0, flags=cb.FLAG_NO_GRAPH)
     for (x, y, r, c), rg, rh in zip(small, g.results, h.results):
-        one = cb.solve_sinkhorn(x, y, r, c, a, 3, 1.0)
+        one = cb.solve_sinkhorn(x, y, r, c, a, 3, 1.0, flags=cb.FLAG_NO_PERSIST)
         assert rg.iterations == one.iterations == rh.iterations
         assert np.array_equal(rg.phi.cpu().numpy(), rh.phi.cpu().numpy())
 
