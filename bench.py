@@ -66,6 +66,9 @@ def parse():
                          "converged potentials, for profiler captures of the steady-state "
                          "kernel; the potentials are solved for and cached in CACHE.npz "
                          "when it does not exist")
+    ap.add_argument("--profile-persist", type=int, default=0, metavar="ITERS",
+                    help="only run one ITERS-iteration Sinkhorn solve of the bench instance "
+                         "(one sk_persist_kernel launch), for profiler captures")
     ap.add_argument("--profile-form", default="fp64", choices=["fp64", "fp32"],
                     help="exponent form of the --profile-pass solve")
     ap.add_argument("--profile-feature", type=int, default=0, metavar="N",
@@ -101,6 +104,28 @@ def profile_steady(args):
         K.warp_logsumexp_ct_fused(X, Y, R, psi, ETA, float(z["winf"]), P, out=phi)
     torch.cuda.synchronize()
     print(json.dumps({"profile_steady": "launched", "finite": bool(torch.isfinite(phi).all())}))
+    return 0
+
+
+def profile_persist(args):
+    """Profiler target for the persistent loop: one solve of the bench instance
+    with epsilon = 0 and itermax = ITERS, i.e. exactly one launch of
+    sk_persist_kernel (`-k regex:sk_persist -c 1`), from converged potentials
+    when `--profile-steady CACHE.npz` names an existing cache."""
+    import numpy as np
+    import torch
+    import culamp_b200 as cb
+    x, y, r, c = instance()
+    X, Y, R, Cc = (torch.as_tensor(v, device="cuda") for v in (x, y, r, c))
+    kw = {}
+    if args.profile_steady and os.path.exists(args.profile_steady):
+        z = np.load(args.profile_steady)
+        kw = {"phi0": torch.as_tensor(z["phi"], device="cuda"), "psi0": torch.as_tensor(z["psi"], device="cuda")}
+    a = cb.EOTArgs(eta_p=ETA, epsilon=0.0, itermax=args.profile_persist, verbose=False)
+    res = cb.solve_sinkhorn(X, Y, R, Cc, a, FREQ, P, **kw)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_persist": args.profile_persist, "iterations": res.iterations,
+                      "loop_ms": res.elapsed_ms, "finite": bool(torch.isfinite(res.phi).all())}))
     return 0
 
 
@@ -323,6 +348,28 @@ def time_pass(torch, K, stream, X, Y, R, pot, out, winf, reps=50, flags=0):
         return e0.elapsed_time(e1) / reps, f"host-launched ({type(ex).__name__})"
 
 
+def kernels_per_call(torch, fn):
+    """(kernel launches, kernel names) of one call, from the CUDA activity
+    profiler; copies and memsets are not kernels. (None, reason) if the
+    profiler is unavailable."""
+    try:
+        from torch.profiler import ProfilerActivity, profile
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            fn()
+            torch.cuda.synchronize()
+        names = []
+        for e in prof.events():
+            if "cuda" not in str(getattr(e, "device_type", "")).lower():
+                continue
+            if e.name.startswith(("Memcpy", "Memset", "cudaMem")):
+                continue
+            names.append(e.name)
+        return len(names), sorted(set(nm.split("(")[0][:80] for nm in names))
+    except Exception as ex:   # profiler missing on this build
+        return None, repr(ex)[:200]
+
+
 def metric_name():
     return "ms to 1e-6 L1 marginal error (kernel Sinkhorn, chosen form)"
 
@@ -341,6 +388,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.profile_persist:
+        return profile_persist(args)
     if args.profile_pass:
         return profile_pass(args)
     if args.profile_feature:
@@ -390,7 +439,7 @@ def main():
     pin = [torch.as_tensor(v).pin_memory() for v in (x, y, r, c)]
     host = [t.numpy() for t in pin]
     cb.solve_sinkhorn(*host, a, FREQ, P)                       # warm the host path
-    times, iters, e2e_t = [], [], []
+    times, loops, iters, e2e_t = [], [], [], []
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             flush.zero_()
@@ -401,6 +450,7 @@ def main():
             e1.record(stream)
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
+            loops.append(res.elapsed_ms)
             iters.append(res.iterations)
             assert res.stopped == 1
             flush.zero_()
@@ -431,38 +481,47 @@ def main():
     h2d = (n * 3 + m * 3 + n + m) * 8
     d2h = (n + m) * 8
 
-    # roofline of the dominant kernel: the fused row-LSE pass at the solve's shape,
-    # updating phi in place (its previous value is the kernel's reference, as in
-    # the solve), launched from a captured CUDA graph and timed with CUDA events
-    psi = res.psi.clone()
-    phi_buf = res.phi.clone()
-    pass_ms, how = time_pass(torch, K, stream, X, Y, R, psi, phi_buf, res.winf, reps=50)
-    pairs = n * m
-    achieved = pairs / (pass_ms * 1e-3)
+    # roofline of the dominant kernel. The solve is one persistent launch of
+    # sk_persist_kernel (every iteration: row pass, column pass, and the check
+    # pass every FREQ iterations); its duration is the solve's loop time
+    # (stats.elapsed_ms: CUDA events around the launch on the solve's stream).
+    loop_ms = statistics.median(loops)
+    checks = 1 + (it_med - 1) // FREQ
+    pairs = (2 * it_med + checks) * n * m
+    achieved = pairs / (loop_ms * 1e-3)
     probe = (C.c_double * 4)()
     h = cb.get_handle(local)
     h.check(h._lib.culamp_probe_pipes(h.ptr, probe, C.c_void_p(stream.cuda_stream)), "probe")
     dfma, ex2, cvt = probe[0], probe[1], probe[2]
-    # per pair of the fixed-reference pass (p = 2, d dims after dropping constant
+    # per pair of the fixed-reference term (p = 2, d dims after dropping constant
     # ones): d DFMA + 1 DADD on the FP64 pipe, 1 ex2 on the XU pipe
     d_eff = 2   # the grid's z coordinate is constant and is dropped
     fp64_bound = dfma / (d_eff + 1.0)
     xu_bound = ex2
     peak = min(fp64_bound, xu_bound)
+    # the same pair pass as one launch of the pass-per-launch loop, for comparison
+    psi = res.psi.clone()
+    phi_buf = res.phi.clone()
+    pass_ms, how = time_pass(torch, K, stream, X, Y, R, psi, phi_buf, res.winf, reps=50)
     roofline = {"bound": "fp64+xu pipes (not hbm/tensor: operands are L2-resident)",
                 "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gpair/s",
                 "frac": achieved / peak,
                 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum):
                 # not measurable without a profiler, so this is the figure of the
-                # last ncu capture of this kernel in its steady state (the
-                # --profile-steady target), named in traffic_source
+                # last ncu capture of this kernel, named in traffic_source
                 "traffic": TRAFFIC_BYTES,
                 "traffic_source": TRAFFIC_SOURCE,
-                "kernel": "pair_pass_kernel<P_SQ,d=2,LSE,R=1,fixed-reference> (fused row LSE)",
-                "per_launch_ms": pass_ms, "pairs_per_launch": pairs, "timing": how,
+                "kernel": "sk_persist_kernel<P_SQ,d=2> (whole Sinkhorn loop, one cooperative launch)",
+                "per_launch_ms": loop_ms, "pairs_per_launch": pairs,
+                "pairs_note": f"{it_med} iterations x 2 passes + {checks} check passes, {n}x{m} pairs each",
+                "timing": "CUDA events around the launch (stats.elapsed_ms), median of the timed solves",
                 "peak_source": "measured in-bench pipe probes (culamp_probe_pipes): "
                                f"DFMA {dfma/1e12:.2f} T/s, ex2 {ex2/1e12:.2f} T/s; "
-                               "peak = min(DFMA/(d+1), ex2) pairs/s, d = 2"}
+                               "peak = min(DFMA/(d+1), ex2) pairs/s, d = 2",
+                "graph_loop_pass": {"ms": pass_ms, "timing": how,
+                                    "gpair_s": n * m / (pass_ms * 1e-3) / 1e9,
+                                    "kernel": "pair_pass_kernel<P_SQ,d=2,LSE,R=1,fixed-reference>, one "
+                                              "row pass of the pass-per-launch loop (FLAG_NO_PERSIST)"}}
 
     line = {"metric": metric_name(), "value": value, "unit": "ms", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": value,
@@ -476,8 +535,17 @@ def main():
                               "with the device-timed solves"},
             "roofline": roofline, "clocks": clk.summary(),
             "gpu_launches": None}
-    # kernel launches per solve: W_inf pass + 3 per iteration (row, column, gated check)
-    line["gpu_launches"] = args.steps * (1 + 3 * it_med + 3)
+    # kernel launches inside the timed region: each step is one device-resident
+    # solve and one host-buffer solve; their kernels are counted on one untimed
+    # solve of each kind with the CUDA activity profiler
+    nd, kd = kernels_per_call(torch, lambda: cb.solve_sinkhorn(X, Y, R, Cc, a, FREQ, P, flags=sflags))
+    nh, kh = kernels_per_call(torch, lambda: cb.solve_sinkhorn(*host, a, FREQ, P))
+    if nd is not None and nh is not None:
+        line["gpu_launches"] = args.steps * (nd + nh)
+        line["gpu_launches_per_solve"] = {"device_inputs": nd, "host_inputs": nh, "kernels": sorted(set(kd + kh))}
+    else:
+        line["gpu_launches"] = None
+        line["gpu_launches_per_solve"] = {"error": kd if nd is None else kh}
 
     if world > 1 and not args.no_extras:
         # every rank takes part (collectives); rank 0 reports

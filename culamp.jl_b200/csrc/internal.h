@@ -147,8 +147,8 @@ cudaError_t launch_pass_batched(const PassParams *plist, const int *block_start,
 
 // ---- whole Sinkhorn loop in one persistent cooperative launch (persist.cu):
 // small problems (p = 1, 2 or Inf with the same cost in the check, d <= 3).
-bool persist_eligible(int n, int m, int d, int pm_iter, int pm_resid);
 int persist_grid(int sm_count, int d, int pm);          // CTAs (0: not launchable)
+bool persist_eligible(int n, int m, int d, int pm_iter, int pm_resid, int grid);
 size_t persist_scratch_bytes(int grid);
 // The loop from the control block's state to its stop; `scratch` holds
 // persist_scratch_bytes(grid) bytes. Completes the control block like the

@@ -10,10 +10,14 @@
 //   * CTA b owns the output rows [b n / G, (b+1) n / G) of each half-step (G =
 //     grid size), so a row's log-sum-exp is finished inside its CTA: no split
 //     partials, no tickets. Its 16 warps spread the columns over their lanes,
-//     four columns per thread in registers, and walk the CTA's rows (14 at a
-//     time, their data broadcast from shared memory). The per-thread column
-//     sums are merged across each warp by a butterfly reduce-scatter and across
-//     the warps in shared memory in a fixed order.
+//     four columns per thread in registers, and walk the CTA's rows (28 at a
+//     time, two per packed FP32x2 accumulator, their data broadcast from a
+//     shared-memory cache of the CTA's rows made at kernel entry). The
+//     per-thread column sums are merged across each warp by a butterfly
+//     reduce-scatter and across the warps in shared memory in a fixed order;
+//     warp 0 finishes the group, one row per lane, with no further barrier.
+//     The CTA is the only writer of its rows' potentials, so it keeps them and
+//     each row's fixed-reference offset in that cache.
 //   * Each term uses the fixed-reference exponent of the pass engine (DADD with
 //     FR_MAGIC, funnel-shifted mantissa, one MUFU ex2, exponent-field add,
 //     scaled by 2^FR_C0). A row whose sum leaves the window is recomputed by one
@@ -33,16 +37,18 @@
 //
 // Potentials written by other CTAs are read with L2-coherent loads (ld.cg).
 
+#include <algorithm>
+
 #include "internal.h"
 
 namespace culamp_dev {
 
 constexpr int PTPB = 512;                  // threads per CTA (one CTA per SM)
 constexpr int PWARPS = PTPB / 32;
-constexpr int PRG = 14;                    // rows per group
+constexpr int PRG = 28;                    // rows per group (warp 0 finishes one row per lane)
+constexpr int PMAXR = 56;                  // rows per CTA and side (2 groups)
 constexpr unsigned long long PERSIST_WAIT_NS = 2000000000ull;
-constexpr int PERSIST_MAX_POINTS = 16384;  // per side: <= 16 terms per thread partial
-constexpr double PERSIST_MAX_PAIRS = 134217728.0;   // 2^27 pairs (8192 x 16384)
+constexpr int PERSIST_MAX_POINTS = 8192;   // per side: <= 16 FP32 terms per thread partial
 
 struct GridBar {
     unsigned count;    // arrivals at the current barrier
@@ -103,34 +109,43 @@ __device__ bool grid_sync(GridBar *gb, unsigned &gen, int *s_flag) {
     return *s_flag != 0;
 }
 
-// One half-step's geometry and coefficients. Rows: the points whose potential
-// is written (X side), columns: the others.
-struct Half {
-    const double *Xr, *Yc;     // row points, column points
-    const double *marg;        // row marginal
-    const double *colpot;      // column potential (read through L2)
-    double *rowpot;            // row potential: reference in, result out
-    int nr, nc;
+// This CTA's rows of one side -- the points whose potential a half-step
+// writes -- cached at kernel entry: constants, the row's potential (this CTA
+// is its only writer) and the fixed-reference offset K of the row's next pass,
+// K = FR_MAGIC - (M2 + 1) with M2 = (previous LSE) * log2(e) - H.
+struct SideRows {
+    double4 xr[PMAXR];         // p = 2: {-2 a2 v, K}; else {v, K}  (v = x - ctr)
+    float4 vf[PMAXR];          // v in FP32 (p = 2 cost moment)
+    double marg[PMAXR], logm[PMAXR];
+    double H[PMAXR];           // a2 |v|^2 for p = 2, else 0
+    double M2[PMAXR];          // the reference the row's K was made from
+    double pot[PMAXR];
 };
 
 struct PShared {
-    double4 row[PRG];          // p = 2: {-2 a2 v, K}; else {v, K} (v = x - ctr)
-    float4 rowf[PRG];          // v in FP32 (p = 2 cost moment)
-    double hm[PRG][2];         // H (a2 |v|^2 for p = 2, else 0), M2 = reference - H (log2 units)
-    float red[PWARPS][16];
-    float redm[PWARPS][16];
-    double L[PRG], E[PRG];     // natural-log LSE, softmax-weighted mean cost
-    int bad[PRG];
-    double con[PRG][3];        // per-row contributions to the CTA's partial sums
+    SideRows side[2];          // 0: the x points (phi), 1: the y points (psi)
+    float red[PWARPS][32];
+    float redm[PWARPS][32];
     int flag;
 };
 
-// Butterfly reduce-scatter of 16 values over a warp: afterwards lane l holds in
-// a[0] the warp total of value l >> 1 (16 shuffles instead of 16 x 5).
-__device__ __forceinline__ void warp_scatter16(float (&a)[16]) {
+// One side of the problem as the rows of a half-step.
+struct Side {
+    const double *pts;         // points (n x D), read-only
+    const double *marg;        // marginal
+    double *pot;               // potential (global: other CTAs read it as columns)
+    int n;
+};
+
+__device__ __forceinline__ int rows_lo(int n) { return (int)(((long long)blockIdx.x * n) / gridDim.x); }
+__device__ __forceinline__ int rows_hi(int n) { return (int)(((long long)(blockIdx.x + 1) * n) / gridDim.x); }
+
+// Butterfly reduce-scatter of 32 values over a warp: afterwards lane l holds in
+// a[0] the warp total of value l (31 shuffles instead of 32 x 5).
+__device__ __forceinline__ void warp_scatter32(float (&a)[32]) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
-    for (int o = 16, L = 16; o >= 2; o >>= 1, L >>= 1) {
+    for (int o = 16, L = 32; o >= 1; o >>= 1, L >>= 1) {
         const bool up = (lane & o) != 0;
 #pragma unroll
         for (int i = 0; i < L / 2; ++i) {
@@ -139,10 +154,9 @@ __device__ __forceinline__ void warp_scatter16(float (&a)[16]) {
             a[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
         }
     }
-    a[0] += __shfl_xor_sync(0xffffffffu, a[0], 1);
 }
 
-// One fixed-reference term from dv = t - Mref - 1 + FR_MAGIC (see the pass
+// One fixed-reference term from dv = t - Mref - 1 + FR_MAGIC (the pass
 // engine's tile_lse_fixedref): 2^(t - Mref) * 2^C0 for t - Mref in
 // [-C0, 126 - C0]. ZLOW: a term below the window becomes a subnormal (< 2^-126)
 // instead of ~2..4, so it adds nothing to a moment -- the check pass's cost
@@ -164,22 +178,23 @@ __device__ __forceinline__ float fr_term(double dv) {
     }
 }
 
-// Exact FP64 online log-sum-exp of one row over all columns, by one warp:
-// the recompute of a row whose fixed-reference sum left the window.
+// Exact FP64 online log-sum-exp of row o over all columns, by one warp (the
+// recompute of a row whose fixed-reference sum left the window). Every lane
+// returns the result.
 template <int PM, int D>
-__device__ void row_lse_exact(const Half &H, int o, double alpha, double inv_winf, double pexp,
-                              double &L, double &Ec) {
+__device__ void row_lse_exact(const double *rows, int o, const double *cols, int nc, const double *colpot,
+                              double alpha, double inv_winf, double pexp, double &L, double &Ec) {
     const int lane = threadIdx.x & 31;
     double xv[D];
 #pragma unroll
-    for (int k = 0; k < D; ++k) xv[k] = H.Xr[(size_t)o * D + k];
+    for (int k = 0; k < D; ++k) xv[k] = rows[(size_t)o * D + k];
     double M = -INFINITY, S = 0.0, MO = 0.0;
-    for (int j = lane; j < H.nc; j += 32) {
+    for (int j = lane; j < nc; j += 32) {
         double yv[D];
 #pragma unroll
-        for (int k = 0; k < D; ++k) yv[k] = H.Yc[(size_t)j * D + k];
+        for (int k = 0; k < D; ++k) yv[k] = cols[(size_t)j * D + k];
         const double cc = pair_cost_direct<PM>(xv, yv, D, pexp);
-        const double t = fma(alpha, cc, __ldcg(H.colpot + j));
+        const double t = fma(alpha, cc, __ldcg(colpot + j));
         const double cn = cc * inv_winf;
         if (t == -INFINITY) continue;
         if (t > M) {
@@ -215,193 +230,217 @@ __device__ void row_lse_exact(const Half &H, int o, double alpha, double inv_win
     Ec = (S > 0.0) ? MO / S * (1.0 / inv_winf) : 0.0;
 }
 
-// Log-sum-exp of one group of up to PRG rows [row0, row0 + nrows) against all
-// columns; leaves L (and with MOM the mean cost) of each row in sh.L / sh.E.
-// Reference of row o: log(marg_o) - rowpot_o, its previous log-sum-exp (the
-// row update) or the one the check's potentials were made from (the check).
+// Kernel-entry set-up of this CTA's rows of one side.
+template <int PM, int D>
+__device__ void cache_side(const Side &s, SideRows &R, const double (&ctr)[D], double a2) {
+    constexpr bool SQ = (PM == P_SQ);
+    const int lo = rows_lo(s.n), cnt = rows_hi(s.n) - lo;
+    for (int i = threadIdx.x; i < PMAXR; i += PTPB) {
+        const bool ok = i < cnt;
+        const int o = lo + i;
+        double v[3] = {0.0, 0.0, 0.0};
+        double h = 0.0;
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            v[k] = ok ? s.pts[(size_t)o * D + k] - ctr[k] : 0.0;
+            h = fma(v[k], v[k], h);
+        }
+        const double Hh = SQ ? a2 * h : 0.0;
+        const double mg = ok ? s.marg[o] : 1.0;
+        const double lm = log(mg);
+        const double pot = ok ? __ldcg(s.pot + o) : 0.0;
+        const double M2 = (lm - pot) * LOG2E - Hh;
+        const double K = FR_MAGIC - (M2 + 1.0);
+        R.xr[i] = SQ ? make_double4(-2.0 * a2 * v[0], -2.0 * a2 * v[1], -2.0 * a2 * v[2], K)
+                     : make_double4(v[0], v[1], v[2], K);
+        R.vf[i] = make_float4((float)v[0], (float)v[1], (float)v[2], 0.f);
+        R.marg[i] = mg;
+        R.logm[i] = lm;
+        R.H[i] = Hh;
+        R.M2[i] = M2;
+        R.pot[i] = pot;
+    }
+}
+
+enum HalfMode { HM_ROW = 0, HM_CHECK = 1 };
+
+// One half-step over this CTA's rows of side s (cached in R) against the
+// columns `cols` (nc points, potential colpot), in groups of PRG rows; warp 0
+// finishes each group (lane r = row r). HM_ROW: the row update of
+// warp_logsumexp_ct_fused! (EPI_SK_ROW): pot = log(marg) - L into R and s.pot,
+// K refreshed; part[0] = sum marg . pot. HM_CHECK: the row residual of
+// residual_opt! (EPI_SK_RESID): part = {sum |marg - mass|, sum mass E[C],
+// sum marg . pot}. part is valid in thread 0, in a fixed summation order.
 template <int PM, int D, bool MOM, int CB>
-__device__ void group_lse(const Half &H, int row0, int nrows, const double (&ctr)[D], double a2,
-                          double inv_winf, double pexp, PShared &sh) {
+__device__ void pass_rows(const Side &s, SideRows &R, const double *cols, int nc, const double *colpot,
+                          const double (&ctr)[D], double a2, double inv_winf, double pexp, int mode,
+                          PShared &sh, double (&part)[3]) {
     constexpr bool SQ = (PM == P_SQ);
     // window exponent: the row update's LSE may move well above its reference
     // (FR_C0 leaves 46 above); the check's hardly moves, and its cost moment
     // wants the small terms
     constexpr int C0 = MOM ? 120 : FR_C0;
+    constexpr int NP = PRG / 2;
     static_assert(CB == 2 || CB == 4, "columns per thread step");
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid < PRG) {
-        const int o = row0 + tid;
-        const bool ok = tid < nrows;
-        double v[3] = {0.0, 0.0, 0.0};
-        double h = 0.0;
-#pragma unroll
-        for (int k = 0; k < D; ++k) {
-            v[k] = ok ? H.Xr[(size_t)o * D + k] - ctr[k] : 0.0;
-            h = fma(v[k], v[k], h);
-        }
-        const double Hh = SQ ? a2 * h : 0.0;
-        const double ref = ok ? log(H.marg[o]) - __ldcg(H.rowpot + o) : 0.0;
-        const double M2 = ref * LOG2E - Hh;
-        sh.row[tid] = SQ ? make_double4(-2.0 * a2 * v[0], -2.0 * a2 * v[1], -2.0 * a2 * v[2], FR_MAGIC - (M2 + 1.0))
-                         : make_double4(v[0], v[1], v[2], FR_MAGIC - (M2 + 1.0));
-        sh.rowf[tid] = make_float4((float)v[0], (float)v[1], (float)v[2], 0.f);
-        sh.hm[tid][0] = Hh;
-        sh.hm[tid][1] = M2;
-    }
-    __syncthreads();
-    unsigned long long acc[PRG], mo[MOM ? PRG : 1];
-#pragma unroll
-    for (int r = 0; r < PRG; ++r) acc[r] = 0ull;
-#pragma unroll
-    for (int r = 0; r < (MOM ? PRG : 1); ++r) mo[r] = 0ull;
+    const int lo = rows_lo(s.n), cnt = rows_hi(s.n) - lo;
     const float invw_f = (float)inv_winf;
-    for (int jb = 0; jb < H.nc; jb += CB * PTPB) {
-        double4 col[CB];
-        float cfy[(MOM && SQ) ? CB : 1][3];
+    part[0] = part[1] = part[2] = 0.0;
+    for (int g0 = 0; g0 < cnt; g0 += PRG) {
+        const int nrows = min(PRG, cnt - g0);
+        unsigned long long acc[NP], mo[MOM ? NP : 1];
 #pragma unroll
-        for (int c = 0; c < CB; ++c) {
-            const int j = jb + c * PTPB + tid;
-            double yy[3] = {0.0, 0.0, 0.0};
-            double g = -INFINITY;
-            if (j < H.nc) {
-                double s2 = 0.0;
+        for (int q = 0; q < NP; ++q) acc[q] = 0ull;
 #pragma unroll
-                for (int k = 0; k < D; ++k) {
-                    yy[k] = H.Yc[(size_t)j * D + k] - ctr[k];
-                    s2 = fma(yy[k], yy[k], s2);
-                }
-                g = LOG2E * __ldcg(H.colpot + j);
-                if (SQ) g += a2 * s2;
-            }
-            col[c] = make_double4(yy[0], yy[1], yy[2], g);
-            if constexpr (MOM && SQ) {
-#pragma unroll
-                for (int k = 0; k < 3; ++k) cfy[c][k] = (float)yy[k];
-            }
-        }
-#pragma unroll
-        for (int r = 0; r < PRG; ++r) {
-            const double4 rd = sh.row[r];
-            float e[CB], cf[CB];
+        for (int q = 0; q < (MOM ? NP : 1); ++q) mo[q] = 0ull;
+        for (int jb = 0; jb < nc; jb += CB * PTPB) {
+            double4 col[CB];
+            float cfy[(MOM && SQ) ? CB : 1][3];
 #pragma unroll
             for (int c = 0; c < CB; ++c) {
-                double t;
-                cf[c] = 0.f;
-                if (SQ) {
-                    t = col[c].w;
-                    if (D >= 3) t = fma(rd.z, col[c].z, t);
-                    if (D >= 2) t = fma(rd.y, col[c].y, t);
-                    t = fma(rd.x, col[c].x, t);
-                } else {
-                    const double xv[3] = {rd.x, rd.y, rd.z};
-                    const double yv[3] = {col[c].x, col[c].y, col[c].z};
-                    const double cc = pair_cost_direct<PM>(xv, yv, D, pexp);
-                    t = fma(cc, a2, col[c].w);
-                    if (MOM) cf[c] = (float)(cc * inv_winf);
+                const int j = jb + c * PTPB + tid;
+                double yy[3] = {0.0, 0.0, 0.0};
+                double g = -INFINITY;
+                if (j < nc) {
+                    double s2 = 0.0;
+#pragma unroll
+                    for (int k = 0; k < D; ++k) {
+                        yy[k] = cols[(size_t)j * D + k] - ctr[k];
+                        s2 = fma(yy[k], yy[k], s2);
+                    }
+                    g = LOG2E * __ldcg(colpot + j);
+                    if (SQ) g += a2 * s2;
                 }
-                e[c] = fr_term<C0, MOM>(t + rd.w);
+                col[c] = make_double4(yy[0], yy[1], yy[2], g);
+                if constexpr (MOM && SQ) {
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) cfy[c][k] = (float)yy[k];
+                }
             }
-            if constexpr (MOM && SQ) {
-                const float4 rf = sh.rowf[r];
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+                const double4 ra = R.xr[g0 + 2 * q], rb = R.xr[g0 + 2 * q + 1];
+                float ea[CB], eb[CB], ca[CB], cbw[CB];
 #pragma unroll
                 for (int c = 0; c < CB; ++c) {
-                    const float d0 = rf.x - cfy[c][0], d1 = rf.y - cfy[c][1], d2 = rf.z - cfy[c][2];
-                    cf[c] = fmaf(d2, d2, fmaf(d1, d1, d0 * d0)) * invw_f;
+                    double ta, tb;
+                    ca[c] = cbw[c] = 0.f;
+                    if (SQ) {
+                        ta = col[c].w;
+                        tb = col[c].w;
+                        if (D >= 3) { ta = fma(ra.z, col[c].z, ta); tb = fma(rb.z, col[c].z, tb); }
+                        if (D >= 2) { ta = fma(ra.y, col[c].y, ta); tb = fma(rb.y, col[c].y, tb); }
+                        ta = fma(ra.x, col[c].x, ta);
+                        tb = fma(rb.x, col[c].x, tb);
+                    } else {
+                        const double xa[3] = {ra.x, ra.y, ra.z}, xb[3] = {rb.x, rb.y, rb.z};
+                        const double yv[3] = {col[c].x, col[c].y, col[c].z};
+                        const double cca = pair_cost_direct<PM>(xa, yv, D, pexp);
+                        const double ccb = pair_cost_direct<PM>(xb, yv, D, pexp);
+                        ta = fma(cca, a2, col[c].w);
+                        tb = fma(ccb, a2, col[c].w);
+                        if (MOM) { ca[c] = (float)(cca * inv_winf); cbw[c] = (float)(ccb * inv_winf); }
+                    }
+                    ea[c] = fr_term<C0, MOM>(ta + ra.w);
+                    eb[c] = fr_term<C0, MOM>(tb + rb.w);
+                }
+                if constexpr (MOM && SQ) {
+                    const float4 fa = R.vf[g0 + 2 * q], fb = R.vf[g0 + 2 * q + 1];
+#pragma unroll
+                    for (int c = 0; c < CB; ++c) {
+                        float d0 = fa.x - cfy[c][0], d1 = fa.y - cfy[c][1], d2 = fa.z - cfy[c][2];
+                        ca[c] = fmaf(d2, d2, fmaf(d1, d1, d0 * d0)) * invw_f;
+                        d0 = fb.x - cfy[c][0]; d1 = fb.y - cfy[c][1]; d2 = fb.z - cfy[c][2];
+                        cbw[c] = fmaf(d2, d2, fmaf(d1, d1, d0 * d0)) * invw_f;
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < CB; ++c) acc[q] = add_f32x2(acc[q], pack_f32x2(ea[c], eb[c]));
+                if constexpr (MOM) {
+#pragma unroll
+                    for (int c = 0; c < CB; ++c)
+                        mo[q] = fma_f32x2(pack_f32x2(ea[c], eb[c]), pack_f32x2(ca[c], cbw[c]), mo[q]);
                 }
             }
-            acc[r] = add_f32x2(acc[r], pack_f32x2(e[0], e[1]));
-            if (CB == 4) acc[r] = add_f32x2(acc[r], pack_f32x2(e[CB == 4 ? 2 : 0], e[CB == 4 ? 3 : 1]));
-            if constexpr (MOM) {
-                mo[r] = fma_f32x2(pack_f32x2(e[0], e[1]), pack_f32x2(cf[0], cf[1]), mo[r]);
-                if (CB == 4)
-                    mo[r] = fma_f32x2(pack_f32x2(e[CB == 4 ? 2 : 0], e[CB == 4 ? 3 : 1]),
-                                      pack_f32x2(cf[CB == 4 ? 2 : 0], cf[CB == 4 ? 3 : 1]), mo[r]);
-            }
         }
-    }
-    {
-        float a[16];
+        {
+            float a[32];
 #pragma unroll
-        for (int r = 0; r < 16; ++r) a[r] = (r < PRG) ? lo_f32(acc[r < PRG ? r : 0]) + hi_f32(acc[r < PRG ? r : 0]) : 0.f;
-        warp_scatter16(a);
-        if ((lane & 1) == 0 && (lane >> 1) < PRG) sh.red[warp][lane >> 1] = a[0];
-    }
-    if constexpr (MOM) {
-        float a[16];
+            for (int q = 0; q < NP; ++q) { a[2 * q] = lo_f32(acc[q]); a[2 * q + 1] = hi_f32(acc[q]); }
 #pragma unroll
-        for (int r = 0; r < 16; ++r) a[r] = (r < PRG) ? lo_f32(mo[r < PRG ? r : 0]) + hi_f32(mo[r < PRG ? r : 0]) : 0.f;
-        warp_scatter16(a);
-        if ((lane & 1) == 0 && (lane >> 1) < PRG) sh.redm[warp][lane >> 1] = a[0];
-    }
-    __syncthreads();
-    if (tid < nrows) {
-        double S = 0.0, MOv = 0.0;
-#pragma unroll
-        for (int w = 0; w < PWARPS; ++w) {
-            S += (double)sh.red[w][tid];
-            if (MOM) MOv += (double)sh.redm[w][tid];
+            for (int i = PRG; i < 32; ++i) a[i] = 0.f;
+            warp_scatter32(a);
+            sh.red[warp][lane] = a[0];
         }
-        // the window: no term clamped high (S <= 2^126 scaled), and the full
-        // sum within C0 - 32 - log2(nc) below the reference (the engine's
-        // fr_low_margin), i.e. log2(S) >= 32 + log2(nc)
-        const bool good = S > 0.0 && S <= FR_SUM_MAX && log2(S) >= 32.0 + log2((double)H.nc);
-        sh.bad[tid] = !good;
-        if (good) {
-            sh.L[tid] = LN2 * (sh.hm[tid][0] + sh.hm[tid][1] + (log2(S) - (double)C0));
-            sh.E[tid] = MOM ? MOv / S / inv_winf : 0.0;
-        }
-    }
-    __syncthreads();
-    for (int rr = warp; rr < nrows; rr += PWARPS) {
-        if (!sh.bad[rr]) continue;
-        double L, Ec;
-        row_lse_exact<PM, D>(H, row0 + rr, a2 * LN2, inv_winf, pexp, L, Ec);
-        if (lane == 0) { sh.L[rr] = L; sh.E[rr] = Ec; }
-    }
-    __syncthreads();
-}
-
-enum HalfMode { HM_ROW = 0, HM_CHECK = 1 };
-
-// One half-step over this CTA's rows. HM_ROW: rowpot = log(marg) - L
-// (EPI_SK_ROW), part[0] = sum marg . rowpot. HM_CHECK: the row residual of
-// residual_opt! (EPI_SK_RESID): part = {sum |marg - mass|, sum mass E[C],
-// sum marg . rowpot}. part is valid in thread 0, summed in row order.
-template <int PM, int D, bool MOM, int CB>
-__device__ void half_step(const Half &H, const double (&ctr)[D], double a2, double inv_winf,
-                          double pexp, int mode, PShared &sh, double (&part)[3]) {
-    const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
-    const int r_lo = (int)(((long long)b * H.nr) / G);
-    const int r_hi = (int)(((long long)(b + 1) * H.nr) / G);
-    part[0] = part[1] = part[2] = 0.0;
-    for (int row0 = r_lo; row0 < r_hi; row0 += PRG) {
-        const int nrows = min(PRG, r_hi - row0);
-        group_lse<PM, D, MOM, CB>(H, row0, nrows, ctr, a2, inv_winf, pexp, sh);
-        if (tid < nrows) {
-            const int o = row0 + tid;
-            const double L = sh.L[tid];
-            if (mode == HM_ROW) {
-                const double v = log(H.marg[o]) - L;
-                H.rowpot[o] = v;
-                sh.con[tid][0] = H.marg[o] * v;
-                sh.con[tid][1] = sh.con[tid][2] = 0.0;
-            } else {
-                const double f = __ldcg(H.rowpot + o);
-                const double mass = exp(f + L);
-                sh.con[tid][0] = fabs(H.marg[o] - mass);
-                sh.con[tid][1] = mass * sh.E[tid];
-                sh.con[tid][2] = H.marg[o] * f;
-            }
+        if constexpr (MOM) {
+            float a[32];
+#pragma unroll
+            for (int q = 0; q < NP; ++q) { a[2 * q] = lo_f32(mo[q]); a[2 * q + 1] = hi_f32(mo[q]); }
+#pragma unroll
+            for (int i = PRG; i < 32; ++i) a[i] = 0.f;
+            warp_scatter32(a);
+            sh.redm[warp][lane] = a[0];
         }
         __syncthreads();
-        if (tid == 0)
-            for (int r = 0; r < nrows; ++r)
-                for (int k = 0; k < 3; ++k) part[k] += sh.con[r][k];
+        if (warp == 0) {
+            const bool valid = lane < nrows;
+            const int il = g0 + (valid ? lane : 0);
+            double S = 0.0, MOv = 0.0;
+#pragma unroll
+            for (int w = 0; w < PWARPS; ++w) {
+                S += (double)sh.red[w][lane];
+                if (MOM) MOv += (double)sh.redm[w][lane];
+            }
+            // the window: no term clamped high (S <= 2^126 scaled), and the full
+            // sum within C0 - 32 - log2(nc) below the reference (the engine's
+            // fr_low_margin), i.e. log2(S) >= 32 + log2(nc)
+            const bool good = S > 0.0 && S <= FR_SUM_MAX && log2(S) >= 32.0 + log2((double)nc);
+            double L = 0.0, E = 0.0;
+            if (valid && good) {
+                L = LN2 * (R.H[il] + R.M2[il] + (log2(S) - (double)C0));
+                E = MOM ? MOv / S / inv_winf : 0.0;
+            }
+            unsigned bad = __ballot_sync(0xffffffffu, valid && !good);
+            while (bad) {
+                const int rr = __ffs(bad) - 1;
+                bad &= bad - 1u;
+                double Lx, Ex;
+                row_lse_exact<PM, D>(s.pts, lo + g0 + rr, cols, nc, colpot, a2 * LN2, inv_winf, pexp, Lx, Ex);
+                if (lane == rr) { L = Lx; E = Ex; }
+            }
+            double c0 = 0.0, c1 = 0.0, c2 = 0.0;
+            if (valid) {
+                const int o = lo + il;
+                if (mode == HM_ROW) {
+                    const double v = R.logm[il] - L;
+                    s.pot[o] = v;
+                    R.pot[il] = v;
+                    const double M2 = L * LOG2E - R.H[il];
+                    R.M2[il] = M2;
+                    R.xr[il].w = FR_MAGIC - (M2 + 1.0);
+                    c0 = R.marg[il] * v;
+                } else {
+                    const double f = R.pot[il];
+                    const double mass = exp(f + L);
+                    c0 = fabs(R.marg[il] - mass);
+                    c1 = mass * E;
+                    c2 = R.marg[il] * f;
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                c0 += __shfl_down_sync(0xffffffffu, c0, off);
+                c1 += __shfl_down_sync(0xffffffffu, c1, off);
+                c2 += __shfl_down_sync(0xffffffffu, c2, off);
+            }
+            if (lane == 0) { part[0] += c0; part[1] += c1; part[2] += c2; }
+        }
+        if (g0 + PRG < cnt) __syncthreads();
     }
 }
 
 // Sum over CTAs of slot k of the per-CTA partials, in CTA order (the same
-// value in every CTA). Thread 0 only.
+// value in every CTA).
 __device__ __forceinline__ double cta_total(const double *blk, int k) {
     double s = 0.0;
     for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(blk + b * 4 + k);
@@ -425,8 +464,11 @@ __global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_consta
     double ctr[D];
 #pragma unroll
     for (int k = 0; k < D; ++k) ctr[k] = P.X[k];
-    const Half rowh{P.X, P.Y, P.r, P.psi, P.phi, P.n, P.m};
-    const Half colh{P.Y, P.X, P.c, P.phi, P.psi, P.m, P.n};
+    const Side sx{P.X, P.r, P.phi, P.n};
+    const Side sy{P.Y, P.c, P.psi, P.m};
+    cache_side<PM, D>(sx, sh.side[0], ctr, a2);
+    cache_side<PM, D>(sy, sh.side[1], ctr, a2);
+    __syncthreads();
     long long iter = ctl->iter, num_iter = ctl->num_iter;
     const long long itermax = ctl->itermax, freq = ctl->frequency;
     const double tol = ctl->epsilon / 6.0;
@@ -437,9 +479,9 @@ __global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_consta
     bool checked = false, failed = false;
     double residual = 0.0, objective = 0.0;
     for (;;) {
-        half_step<PM, D, false, 4>(rowh, ctr, a2, inv_winf, P.pexp, HM_ROW, sh, part);
+        pass_rows<PM, D, false, 4>(sx, sh.side[0], P.Y, P.m, P.psi, ctr, a2, inv_winf, P.pexp, HM_ROW, sh, part);
         if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
-        half_step<PM, D, false, 4>(colh, ctr, a2, inv_winf, P.pexp, HM_ROW, sh, part);
+        pass_rows<PM, D, false, 4>(sy, sh.side[1], P.X, P.n, P.phi, ctr, a2, inv_winf, P.pexp, HM_ROW, sh, part);
         if (tid == 0) {
             P.blk[b * 4 + 0] = part[0];
             if (b == 0) {
@@ -459,7 +501,7 @@ __global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_consta
             if (pending) { stop_reason = pending; break; }
             continue;
         }
-        half_step<PM, D, true, 2>(rowh, ctr, a2, inv_winf, P.pexp, HM_CHECK, sh, part);
+        pass_rows<PM, D, true, 2>(sx, sh.side[0], P.Y, P.m, P.psi, ctr, a2, inv_winf, P.pexp, HM_CHECK, sh, part);
         if (tid == 0) {
             P.blk[b * 4 + 1] = part[0];
             P.blk[b * 4 + 2] = part[1];
@@ -505,17 +547,19 @@ __global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_consta
 
 }  // namespace culamp_dev
 
+
 namespace culamp_host {
 
 using namespace culamp_dev;
 
-bool persist_eligible(int n, int m, int d, int pm_iter, int pm_resid) {
+bool persist_eligible(int n, int m, int d, int pm_iter, int pm_resid, int grid) {
     if (pm_iter != pm_resid) return false;
     if (pm_iter != P_L1 && pm_iter != P_SQ && pm_iter != P_INF) return false;
-    if (d < 1 || d > MAXD_PACKED) return false;
-    // each thread's FP32 partial covers at most 16 terms per packed half
+    if (d < 1 || d > MAXD_PACKED || grid < 1) return false;
+    // each thread's FP32 partial of a row covers at most 16 terms
     if (n > PERSIST_MAX_POINTS || m > PERSIST_MAX_POINTS) return false;
-    return (double)n * (double)m <= PERSIST_MAX_PAIRS;
+    // every CTA's rows of both sides fit its shared-memory row cache
+    return (std::max(n, m) + grid - 1) / grid <= PMAXR;
 }
 
 size_t persist_scratch_bytes(int grid) {

@@ -564,8 +564,9 @@ int sinkhorn_loop(culamp_handle h, int n, int m, int d, double p, double eta, do
         return iteration(s, with_check);
     };
     const bool persist = !(flags & (CULAMP_FLAG_NO_GRAPH | CULAMP_FLAG_NO_PERSIST)) && !pl.ladder &&
-                         !pl.k1.fp32 && !S.feat_active && persist_eligible(n, m, d, pl.pm_iter, pl.pm_resid);
-    const int pgrid = persist ? persist_grid(h->sm_count, d, pl.pm_iter) : 0;
+                         !pl.k1.fp32 && !S.feat_active && d <= MAXD_PACKED;
+    int pgrid = persist ? persist_grid(h->sm_count, d, pl.pm_iter) : 0;
+    if (pgrid > 0 && !persist_eligible(n, m, d, pl.pm_iter, pl.pm_resid, pgrid)) pgrid = 0;
     if (pgrid > 0) CUDA_TRY(h, S.pers.reserve(persist_scratch_bytes(pgrid)));
     CUDA_TRY(h, cudaEventRecord(S.ev0, st));
     bool ran = false;

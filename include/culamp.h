@@ -68,8 +68,8 @@ extern "C" {
                                           take the precision ladder.                        */
 #define CULAMP_FLAG_NO_PERSIST  1024u  /* Sinkhorn: one launch per pass (CUDA graph) instead of the
                                           whole loop in one persistent launch, which small
-                                          problems (n, m <= 16384, n m <= 2^27, d <= 3,
-                                          p = 1, 2 or Inf) take by default                  */
+                                          problems (n, m <= 8192, d <= 3, p = 1, 2 or Inf)
+                                          take by default                                   */
 #define CULAMP_FLAG_FEAT_FP64     64u  /* feature clouds on the FP64 pair loops instead of
                                           the tensor cores (exact inner products, slow)     */
 

@@ -95,7 +95,7 @@ def test_tmax_stops_after_the_first_iteration(grid):
 
 
 @pytest.mark.parametrize("n,m,d", [(5, 7, 3), (1000, 3000, 3), (2500, 1200, 2), (777, 1500, 1),
-                                   (8192, 16384, 3)])
+                                   (8192, 8192, 3), (8192, 16384, 3)])
 def test_ragged_shapes(n, m, d):
     import torch
     import culamp_b200 as cb
