@@ -34,14 +34,17 @@ sys.path.insert(0, os.path.join(ROOT, "culamp.jl_b200"))
 
 ETA = 1e-3
 EPS = 6e-6
-# what the solve computes in: each exponent alpha*C + beta*pot and its max shift
-# in FP64, 2^u on the FP32 MUFU pipe, FP32 chunk sums merged with Kahan
-# compensation, FP64 potentials, marginals and scalar reductions
-DTYPE = "mixed: f64 exponent, f32 ex2 + compensated f32 sums, f64 potentials/reductions"
-# DRAM bytes of one steady-state row pass at 4096^2, from ncu (see traffic_source)
-TRAFFIC_BYTES = 1944576
-TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of "
-                  "`bench.py --profile-steady`, profiles/pair_pass_kernel_row_lse_grid4096_steady.md")
+# what the solve computes in: each exponent alpha*C + beta*pot relative to the
+# row's reference in FP64, 2^u on the FP32 MUFU pipe, short FP32 partial sums
+# (<= 16 terms) merged in FP64, FP64 potentials, marginals and scalar reductions
+DTYPE = "mixed: f64 exponent, f32 ex2 + short f32 partial sums merged in f64, f64 potentials/reductions"
+# DRAM bytes of the persistent loop's launch (the roofline kernel), from ncu
+# (see traffic_source): the instance and potentials are read from DRAM once and
+# stay in L2, so the figure does not grow with the iteration count
+TRAFFIC_BYTES = 429824
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the sk_persist_kernel launch of "
+                  "`bench.py --profile-persist 200` (200 iterations of the bench instance), "
+                  "profiles/sk_persist_kernel_grid4096.md")
 FREQ = 10
 ITERMAX = 200_000
 P = 2.0
@@ -672,12 +675,17 @@ def divergence_extra(cb, D, torch, dev, X, Y, R, Cc, winf_xy):
     e[0].record()
     parts = sinkhorn_divergence(X, Y, R, Cc, eps, P, tol=1e-6, frequency=25)
     e[1].record()
+    e[1].synchronize()
+    forward_ms = e[0].elapsed_time(e[1])
+    divergence_grads(X, Y, parts, P)        # first call: scratch and kernel loading, untimed
+    torch.cuda.synchronize()
+    e[1].record()
     gx, gy, ga, gb = divergence_grads(X, Y, parts, P)
     e[2].record()
     e[2].synchronize()
     grad_ms = e[1].elapsed_time(e[2])
     pairs = 6.0 * X.shape[0] * Y.shape[0]
-    return {"eps": eps, "value": parts.value, "forward_ms": e[0].elapsed_time(e[1]),
+    return {"eps": eps, "value": parts.value, "forward_ms": forward_ms,
             "iterations": [parts.xy.iterations, parts.xx.iterations, parts.yy.iterations],
             "residuals": [parts.xy.residual, parts.xx.residual, parts.yy.residual],
             "adjoint_ms": grad_ms, "adjoint_gpair_s": pairs / (grad_ms * 1e-3) / 1e9,

@@ -147,6 +147,7 @@ cudaError_t launch_pass_batched(const PassParams *plist, const int *block_start,
 
 // ---- whole Sinkhorn loop in one persistent cooperative launch (persist.cu):
 // small problems (p = 1, 2 or Inf with the same cost in the check, d <= 3).
+constexpr int PERSIST_MAX_POINTS = 8192;   // per side: <= 16 FP32 terms per thread partial
 int persist_grid(int sm_count, int d, int pm);          // CTAs (0: not launchable)
 bool persist_eligible(int n, int m, int d, int pm_iter, int pm_resid, int grid);
 size_t persist_scratch_bytes(int grid);

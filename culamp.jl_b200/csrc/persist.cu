@@ -48,7 +48,6 @@ constexpr int PWARPS = PTPB / 32;
 constexpr int PRG = 28;                    // rows per group (warp 0 finishes one row per lane)
 constexpr int PMAXR = 56;                  // rows per CTA and side (2 groups)
 constexpr unsigned long long PERSIST_WAIT_NS = 2000000000ull;
-constexpr int PERSIST_MAX_POINTS = 8192;   // per side: <= 16 FP32 terms per thread partial
 
 struct GridBar {
     unsigned count;    // arrivals at the current barrier
@@ -116,6 +115,7 @@ __device__ bool grid_sync(GridBar *gb, unsigned &gen, int *s_flag) {
 struct SideRows {
     double4 xr[PMAXR];         // p = 2: {-2 a2 v, K}; else {v, K}  (v = x - ctr)
     float4 vf[PMAXR];          // v in FP32 (p = 2 cost moment)
+    float4 xf[PMAXR];          // p = 2, FP32-exponent passes: {-2 a2 v, -M2} in FP32
     double marg[PMAXR], logm[PMAXR];
     double H[PMAXR];           // a2 |v|^2 for p = 2, else 0
     double M2[PMAXR];          // the reference the row's K was made from
@@ -254,6 +254,8 @@ __device__ void cache_side(const Side &s, SideRows &R, const double (&ctr)[D], d
         R.xr[i] = SQ ? make_double4(-2.0 * a2 * v[0], -2.0 * a2 * v[1], -2.0 * a2 * v[2], K)
                      : make_double4(v[0], v[1], v[2], K);
         R.vf[i] = make_float4((float)v[0], (float)v[1], (float)v[2], 0.f);
+        R.xf[i] = make_float4((float)(-2.0 * a2 * v[0]), (float)(-2.0 * a2 * v[1]), (float)(-2.0 * a2 * v[2]),
+                              (float)(-M2));
         R.marg[i] = mg;
         R.logm[i] = lm;
         R.H[i] = Hh;
@@ -271,7 +273,7 @@ enum HalfMode { HM_ROW = 0, HM_CHECK = 1 };
 // K refreshed; part[0] = sum marg . pot. HM_CHECK: the row residual of
 // residual_opt! (EPI_SK_RESID): part = {sum |marg - mass|, sum mass E[C],
 // sum marg . pot}. part is valid in thread 0, in a fixed summation order.
-template <int PM, int D, bool MOM, int CB>
+template <int PM, int D, bool MOM, int CB, bool F32 = false>
 __device__ void pass_rows(const Side &s, SideRows &R, const double *cols, int nc, const double *colpot,
                           const double (&ctr)[D], double a2, double inv_winf, double pexp, int mode,
                           PShared &sh, double (&part)[3]) {
@@ -282,6 +284,7 @@ __device__ void pass_rows(const Side &s, SideRows &R, const double *cols, int nc
     constexpr int C0 = MOM ? 120 : FR_C0;
     constexpr int NP = PRG / 2;
     static_assert(CB == 2 || CB == 4, "columns per thread step");
+    static_assert(!F32 || (SQ && !MOM), "the FP32-exponent pass is the p = 2 row update");
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int lo = rows_lo(s.n), cnt = rows_hi(s.n) - lo;
     const float invw_f = (float)inv_winf;
@@ -293,6 +296,49 @@ __device__ void pass_rows(const Side &s, SideRows &R, const double *cols, int nc
         for (int q = 0; q < NP; ++q) acc[q] = 0ull;
 #pragma unroll
         for (int q = 0; q < (MOM ? NP : 1); ++q) mo[q] = 0ull;
+        if constexpr (F32) {
+            // the exponent in FP32 (the pass engine's tile_lse_fr32): t - Mref =
+            // g_j - M2_i + xr_i . y_j with packed FP32x2 FMAs over the row pair,
+            // 2^(t - Mref) by one MUFU ex2, no window clamp (a sum above 2^64 or
+            // far below the reference takes the exact row)
+            for (int jb = 0; jb < nc; jb += CB * PTPB) {
+                unsigned long long gy[CB], y0[CB], y1[CB], y2[CB];
+#pragma unroll
+                for (int c = 0; c < CB; ++c) {
+                    const int j = jb + c * PTPB + tid;
+                    float yf[3] = {0.f, 0.f, 0.f};
+                    float g = -INFINITY;
+                    if (j < nc) {
+                        double s2 = 0.0;
+#pragma unroll
+                        for (int k = 0; k < D; ++k) {
+                            const double yy = cols[(size_t)j * D + k] - ctr[k];
+                            s2 = fma(yy, yy, s2);
+                            yf[k] = (float)yy;
+                        }
+                        g = (float)(LOG2E * __ldcg(colpot + j) + a2 * s2);
+                    }
+                    gy[c] = pack_f32x2(g, g);
+                    y0[c] = pack_f32x2(yf[0], yf[0]);
+                    y1[c] = pack_f32x2(yf[1], yf[1]);
+                    y2[c] = pack_f32x2(yf[2], yf[2]);
+                }
+#pragma unroll
+                for (int q = 0; q < NP; ++q) {
+                    const float4 fa = R.xf[g0 + 2 * q], fb = R.xf[g0 + 2 * q + 1];
+                    const unsigned long long x0 = pack_f32x2(fa.x, fb.x), x1 = pack_f32x2(fa.y, fb.y);
+                    const unsigned long long x2 = pack_f32x2(fa.z, fb.z), k2 = pack_f32x2(fa.w, fb.w);
+#pragma unroll
+                    for (int c = 0; c < CB; ++c) {
+                        unsigned long long t = add_f32x2(gy[c], k2);
+                        if (D >= 3) t = fma_f32x2(x2, y2[c], t);
+                        if (D >= 2) t = fma_f32x2(x1, y1[c], t);
+                        t = fma_f32x2(x0, y0[c], t);
+                        acc[q] = add_f32x2(acc[q], pack_f32x2(ex2_approx(lo_f32(t)), ex2_approx(hi_f32(t))));
+                    }
+                }
+            }
+        } else
         for (int jb = 0; jb < nc; jb += CB * PTPB) {
             double4 col[CB];
             float cfy[(MOM && SQ) ? CB : 1][3];
@@ -394,10 +440,12 @@ __device__ void pass_rows(const Side &s, SideRows &R, const double *cols, int nc
             // the window: no term clamped high (S <= 2^126 scaled), and the full
             // sum within C0 - 32 - log2(nc) below the reference (the engine's
             // fr_low_margin), i.e. log2(S) >= 32 + log2(nc)
-            const bool good = S > 0.0 && S <= FR_SUM_MAX && log2(S) >= 32.0 + log2((double)nc);
+            // FP32 exponents: unscaled terms, the engine's 2^64 / FR32_LOW_MARGIN window
+            const bool good = F32 ? (S > 0.0 && S <= 0x1p64 && log2(S) >= -FR32_LOW_MARGIN)
+                                  : (S > 0.0 && S <= FR_SUM_MAX && log2(S) >= 32.0 + log2((double)nc));
             double L = 0.0, E = 0.0;
             if (valid && good) {
-                L = LN2 * (R.H[il] + R.M2[il] + (log2(S) - (double)C0));
+                L = LN2 * (R.H[il] + R.M2[il] + (log2(S) - (F32 ? 0.0 : (double)C0)));
                 E = MOM ? MOv / S / inv_winf : 0.0;
             }
             unsigned bad = __ballot_sync(0xffffffffu, valid && !good);
@@ -418,6 +466,7 @@ __device__ void pass_rows(const Side &s, SideRows &R, const double *cols, int nc
                     const double M2 = L * LOG2E - R.H[il];
                     R.M2[il] = M2;
                     R.xr[il].w = FR_MAGIC - (M2 + 1.0);
+                    R.xf[il].w = (float)(-M2);
                     c0 = R.marg[il] * v;
                 } else {
                     const double f = R.pot[il];
@@ -478,10 +527,27 @@ __global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_consta
     int stop_reason = 0;
     bool checked = false, failed = false;
     double residual = 0.0, objective = 0.0;
+    // precision ladder (p = 2): FP32-exponent row and column passes while the
+    // phase lasts; it ends, the same way in every CTA, at the first check whose
+    // FP64 residual is within ctl->ladder_switch or not below the previous one
+    bool fp32_phase = (PM == P_SQ) && ctl->fp32_phase;
+    double ladder_prev = ctl->ladder_prev;
+    const double ladder_switch = ctl->ladder_switch;
     for (;;) {
-        pass_rows<PM, D, false, 4>(sx, sh.side[0], P.Y, P.m, P.psi, ctr, a2, inv_winf, P.pexp, HM_ROW, sh, part);
-        if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
-        pass_rows<PM, D, false, 4>(sy, sh.side[1], P.X, P.n, P.phi, ctr, a2, inv_winf, P.pexp, HM_ROW, sh, part);
+        if constexpr (PM == P_SQ) {
+            if (fp32_phase) {
+                pass_rows<PM, D, false, 4, true>(sx, sh.side[0], P.Y, P.m, P.psi, ctr, a2, inv_winf, P.pexp,
+                                                 HM_ROW, sh, part);
+                if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
+                pass_rows<PM, D, false, 4, true>(sy, sh.side[1], P.X, P.n, P.phi, ctr, a2, inv_winf, P.pexp,
+                                                 HM_ROW, sh, part);
+            }
+        }
+        if (!fp32_phase) {
+            pass_rows<PM, D, false, 4>(sx, sh.side[0], P.Y, P.m, P.psi, ctr, a2, inv_winf, P.pexp, HM_ROW, sh, part);
+            if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
+            pass_rows<PM, D, false, 4>(sy, sh.side[1], P.X, P.n, P.phi, ctr, a2, inv_winf, P.pexp, HM_ROW, sh, part);
+        }
         if (tid == 0) {
             P.blk[b * 4 + 0] = part[0];
             if (b == 0) {
@@ -522,6 +588,8 @@ __global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_consta
         checked = true;
         residual = s_tot[1];
         objective = s_tot[2];
+        if (fp32_phase && (residual <= ladder_switch || residual >= LADDER_STALL * ladder_prev)) fp32_phase = false;
+        ladder_prev = residual;
         if (s_stop != 1) num_iter += 1;
         if (s_stop) { stop_reason = s_stop; break; }
     }
@@ -539,6 +607,8 @@ __global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_consta
     ctl->stop = 1;
     ctl->stop_reason = stop_reason;
     ctl->pending_stop = (stop_reason >= 2) ? stop_reason : 0;
+    ctl->fp32_phase = fp32_phase ? 1 : 0;
+    ctl->ladder_prev = ladder_prev;
     if (checked) {
         ctl->residual = residual;
         ctl->objective = objective;

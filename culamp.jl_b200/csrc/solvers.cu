@@ -437,9 +437,11 @@ struct SkPlan {
 };
 
 // Sinkhorn solves of at least this many pairs take the precision ladder unless
-// CULAMP_FLAG_FORM_FP64 is set. Below it the passes are latency-bound and the
-// FP32-exponent passes save nothing: at 4096^2 the ladder took 86.7 ms against
-// 83.9 ms in FP64, at 65536^2 2.87 s against 4.11 s (same 1e-6 FP64 check).
+// CULAMP_FLAG_FORM_FP64 is set. Below it the default stays the FP64-exponent
+// form, whose iterates follow the reference's step for step; the ladder there
+// is CULAMP_FLAG_LADDER (in the persistent loop, where switching form costs
+// nothing). At 4096^2 the graph-loop ladder took 86.7 ms against 83.9 ms in
+// FP64, at 65536^2 2.87 s against 4.11 s (same 1e-6 FP64 check).
 constexpr double LADDER_AUTO_PAIRS = 268435456.0;   // 16384^2
 
 // The FP32-exponent forms (FORM_FP32, LADDER) exist for the packed p = 2 passes.
@@ -563,8 +565,8 @@ int sinkhorn_loop(culamp_handle h, int n, int m, int d, double p, double eta, do
         body_pos = (body_pos + 1) % unroll;
         return iteration(s, with_check);
     };
-    const bool persist = !(flags & (CULAMP_FLAG_NO_GRAPH | CULAMP_FLAG_NO_PERSIST)) && !pl.ladder &&
-                         !pl.k1.fp32 && !S.feat_active && d <= MAXD_PACKED;
+    const bool persist = !(flags & (CULAMP_FLAG_NO_GRAPH | CULAMP_FLAG_NO_PERSIST)) && !pl.k1.fp32 &&
+                         !S.feat_active && d <= MAXD_PACKED;
     int pgrid = persist ? persist_grid(h->sm_count, d, pl.pm_iter) : 0;
     if (pgrid > 0 && !persist_eligible(n, m, d, pl.pm_iter, pl.pm_resid, pgrid)) pgrid = 0;
     if (pgrid > 0) CUDA_TRY(h, S.pers.reserve(persist_scratch_bytes(pgrid)));

@@ -135,3 +135,30 @@ def test_annealed_solve_uses_the_same_loop(grid):
     ref = cb.solve_annealed_sinkhorn(*grid, cb.EOTArgs(**kw), frequency=10, p=2.0, flags=cb.FLAG_NO_PERSIST)
     assert per.iterations == ref.iterations and per.num_iter == ref.num_iter
     close(per.phi, ref.phi)
+
+
+def test_ladder_in_the_persistent_loop(grid):
+    """CULAMP_FLAG_LADDER in the persistent loop: FP32-exponent row and column
+    passes until a check's FP64 residual is within 32x the tolerance, then the
+    FP64 passes; the stop is decided by FP64 checks only, and the result is the
+    FP64 form's fixed point to the solve's accuracy."""
+    import culamp_b200 as cb
+    x, y, r, c = grid
+    a = cb.EOTArgs(eta_p=1e-3, epsilon=6e-6, itermax=20000, verbose=True)
+    f64 = cb.solve_sinkhorn(x, y, r, c, a, 10, 2.0)
+    lad = cb.solve_sinkhorn(x, y, r, c, a, 10, 2.0, flags=cb.FLAG_LADDER)
+    glad = cb.solve_sinkhorn(x, y, r, c, a, 10, 2.0, flags=cb.FLAG_LADDER | cb.FLAG_NO_PERSIST)
+    print(f"4096 ladder: persistent {lad.elapsed_ms:.2f} ms / {lad.iterations} it, graph loop "
+          f"{glad.elapsed_ms:.2f} ms / {glad.iterations} it, FP64 persistent {f64.elapsed_ms:.2f} ms / "
+          f"{f64.iterations} it")
+    for res in (lad, glad):
+        assert res.stopped == 1 and res.residual <= 1e-6
+        rl, cl = cb.marginal_error_fp64(x, y, r, c, res.phi, res.psi, 1e-3, res.winf, 2.0)
+        assert rl <= 1e-6 and cl <= 1e-6
+        assert abs(res.iterations - f64.iterations) <= 0.05 * f64.iterations + 20
+    rr = _np(r)
+    k0 = np.dot(rr, _np(f64.phi)) / rr.sum()
+    k1 = np.dot(rr, _np(lad.phi)) / rr.sum()
+    scale = max(1.0, np.abs(_np(f64.phi)).max())
+    assert np.abs((_np(lad.phi) - k1) - (_np(f64.phi) - k0)).max() <= 1e-5 * scale
+    assert np.abs((_np(lad.psi) + k1) - (_np(f64.psi) + k0)).max() <= 1e-5 * scale
