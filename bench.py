@@ -39,11 +39,11 @@ EPS = 6e-6
 # (<= 16 terms) merged in FP64, FP64 potentials, marginals and scalar reductions
 DTYPE = "mixed: f64 exponent, f32 ex2 + short f32 partial sums merged in f64, f64 potentials/reductions"
 # DRAM bytes of the persistent loop's launch (the roofline kernel), from ncu
-# (see traffic_source): the instance and potentials are read from DRAM once and
-# stay in L2, so the figure does not grow with the iteration count
-TRAFFIC_BYTES = 429824
+# (see traffic_source): the instance and potentials stay in L2 between
+# iterations, so the figure is a small fraction of the pairs' operand bytes
+TRAFFIC_BYTES = 2014976
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the sk_persist_kernel launch of "
-                  "`bench.py --profile-persist 200` (200 iterations of the bench instance), "
+                  "`bench.py --profile-persist 1711` (the bench solve's 1711 iterations), "
                   "profiles/sk_persist_kernel_grid4096.md")
 FREQ = 10
 ITERMAX = 200_000

@@ -50,11 +50,11 @@ constexpr int PMAXR = 56;                  // rows per CTA and side (2 groups)
 constexpr unsigned long long PERSIST_WAIT_NS = 2000000000ull;
 
 struct GridBar {
-    unsigned count;    // arrivals at the current barrier
-    unsigned gen;      // completed barriers
-    unsigned abort;    // set by a CTA that gave up waiting
-    unsigned tmax_hit; // CTA 0's clock decision for the current iteration
+    unsigned long long count;   // arrivals since the launch (+ PERSIST_ABORT once a CTA gave up)
+    unsigned tmax_hit;          // CTA 0's clock decision for the current iteration
+    unsigned pad;
 };
+constexpr unsigned long long PERSIST_ABORT = 1ull << 62;
 
 struct PersistParams {
     const double *X, *Y;       // point clouds (n x d, m x d), read-only
@@ -72,35 +72,44 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void red_release_add_u64(unsigned long long *p, unsigned long long v) {
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+}
 
-// Grid-wide barrier with a bounded wait. Returns false (in every thread of the
-// CTA) when this CTA gave up or saw another CTA give up.
+// Grid-wide barrier k (k = 0, 1, ... counted by `gen`) with a bounded wait.
+// The arrival counter only grows: barrier k is complete once it reaches
+// (k + 1) G. An arrival is one release-reduction (no round trip), the wait
+// polls the counter with acquire loads; bar.sync before the arrival and after
+// the wait extends both to the whole CTA. A CTA that gives up after
+// PERSIST_WAIT_NS adds PERSIST_ABORT, which every waiter sees at once.
+// Returns false (in every thread of the CTA) when this CTA gave up or saw
+// another CTA give up.
 __device__ bool grid_sync(GridBar *gb, unsigned &gen, int *s_flag) {
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        __threadfence();
-        const unsigned g = gen;
-        if (atomicAdd(&gb->count, 1u) == gridDim.x - 1u) {
-            atomicExch(&gb->count, 0u);
-            __threadfence();
-            atomicExch(&gb->gen, g + 1u);
-        } else {
-            const unsigned long long t0 = globaltimer_ns();
-            unsigned spins = 0;
-            while (ld_acquire_u32(&gb->gen) == g) {
-                if (ld_acquire_u32(&gb->abort)) { ok = 0; break; }
-                if (++spins > 64u) {
-                    if (globaltimer_ns() - t0 > PERSIST_WAIT_NS) {
-                        atomicExch(&gb->abort, 1u);
-                        ok = 0;
-                        break;
-                    }
-                    __nanosleep(64);
+        red_release_add_u64(&gb->count, 1ull);
+        const unsigned long long target = (unsigned long long)(gen + 1u) * gridDim.x;
+        unsigned long long t0 = 0;
+        for (unsigned spins = 0;; ++spins) {
+            const unsigned long long v = ld_acquire_u64(&gb->count);
+            if (v >= PERSIST_ABORT) { ok = 0; break; }
+            if (v >= target) break;
+            if ((spins & 63u) == 63u) {
+                const unsigned long long t = globaltimer_ns();
+                if (t0 == 0) t0 = t;
+                else if (t - t0 > PERSIST_WAIT_NS) {
+                    red_release_add_u64(&gb->count, PERSIST_ABORT);
+                    ok = 0;
+                    break;
                 }
             }
         }
-        __threadfence();
         *s_flag = ok;
     }
     gen += 1u;
@@ -496,6 +505,24 @@ __device__ __forceinline__ double cta_total(const double *blk, int k) {
     return s;
 }
 
+// The four slot totals over CTAs by one warp: lane l sums CTAs l, l + 32, ...
+// in order, then a fixed butterfly -- the same values in every CTA, since every
+// CTA runs the same steps on the same data. Valid in every lane.
+__device__ __forceinline__ void cta_totals4(const double *blk, double (&tot)[4]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) tot[k] = 0.0;
+    for (int b = lane; b < (int)gridDim.x; b += 32) {
+        const double2 v0 = __ldcg(reinterpret_cast<const double2 *>(blk + b * 4));
+        const double2 v1 = __ldcg(reinterpret_cast<const double2 *>(blk + b * 4 + 2));
+        tot[0] += v0.x; tot[1] += v0.y; tot[2] += v1.x; tot[3] += v1.y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) tot[k] += __shfl_xor_sync(0xffffffffu, tot[k], o);
+}
+
 // The Sinkhorn loop (SinkhornKernel.jl:477-559): row update, column update,
 // and every `frequency` iterations the residual check, until the tolerance,
 // itermax or tmax stops it; the control step of each iteration as in
@@ -575,8 +602,13 @@ __global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_consta
         }
         if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
         // FIN_SK_CHECK, the same in every CTA
+        if (tid < 32) {
+            double t4[4];
+            cta_totals4(P.blk, t4);
+            if (tid == 0)
+                for (int k = 0; k < 4; ++k) s_tot[k] = t4[k];
+        }
         if (tid == 0) {
-            for (int k = 0; k < 4; ++k) s_tot[k] = cta_total(P.blk, k);
             const double l1 = s_tot[1];
             int st = 0;
             if (l1 <= tol) st = 1;
