@@ -645,7 +645,14 @@ def extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_chosen, chosen_ms):
     l5 = cb.solve_lamp(X5, Y5, R5, C5, bl, 25, P, flags=cb.FLAG_CHECK_ALWAYS)
     gap = (l5.log[-1][4] - l5.log[-1][5]) if l5.log else float("nan")
     ex["lamp_65536"] = {"reached_tol": l5.stopped == 1, "ms": l5.elapsed_ms, "iterations": l5.iterations,
-                        "residual": l5.residual, "gap": gap, "stop_rule": "gap and marginal"}
+                        "residual": l5.residual, "gap": gap, "stop_rule": "gap and marginal",
+                        "form": "FP32 -> FP64 ladder (the default at >= 16384^2 pairs with checks)"}
+    rl5, cl5 = cb.marginal_error_fp64(X5, Y5, R5, C5, l5.phi, l5.psi, 2.0 * l5.eta_t / l5.s_t, l5.winf, P)
+    ex["lamp_65536"].update({"fp64_row_l1": rl5, "fp64_col_l1": cl5})
+    f5 = cb.solve_lamp(X5, Y5, R5, C5, bl, 25, P, flags=cb.FLAG_CHECK_ALWAYS | cb.FLAG_FORM_FP64)
+    ex["lamp_65536_fp64_form"] = {"reached_tol": f5.stopped == 1, "ms": f5.elapsed_ms, "iterations": f5.iterations,
+                                  "residual": f5.residual,
+                                  "chosen_over_this": (f5.elapsed_ms / l5.elapsed_ms) if l5.stopped == 1 else None}
     # the plain FP32 form of the same LAMP solve (same stopping rule, capped at
     # twice the chosen form's iterations and 30 s)
     pl5 = cb.solve_lamp(X5, Y5, R5, C5, bl.copy(itermax=2 * max(1, l5.iterations), tmax=30.0), 25, P,

@@ -90,17 +90,28 @@ enum Finish {
     FIN_SK_SYM = 9,      // symmetric Sinkhorn pass: tolerance test, iteration bookkeeping
 };
 
-// Precision ladder stall test: a check whose residual is not below this
-// fraction of the previous check's leaves the FP32-exponent phase. Sinkhorn at
-// eta_p = 1e-3 gains only ~7 % per 10 iterations, so the test is plain
-// non-decrease: at the FP32 floor the residual wanders up and down.
-constexpr double LADDER_STALL = 1.0;
+// Precision ladder stall test: the FP32-exponent phase ends after this many
+// consecutive checks without a new lowest residual (at the FP32 floor the
+// residual wanders up and down; LAMP's also rises now and then early on).
+constexpr int LADDER_PATIENCE = 3;
+
+// One FP64 check of the FP32-exponent phase: ends the phase once the residual
+// is within ladder_switch, or has not improved for LADDER_PATIENCE checks.
+__device__ __forceinline__ void ladder_check(int &phase, double &best, int &bad, double l1, double sw) {
+    if (!phase) return;
+    if (l1 < best) { best = l1; bad = 0; }
+    else bad += 1;
+    if (l1 <= sw || bad >= LADDER_PATIENCE) phase = 0;
+}
 
 // Gate: when the kernel runs.
-enum Gate {
-    GATE_ALWAYS = 0, GATE_CHECK = 1, GATE_NOCHECK = 2,
-    GATE_FP32 = 3,       // precision ladder: runs while ctl->fp32_phase is set
-    GATE_FP64 = 4,       // precision ladder: runs once ctl->fp32_phase is cleared
+enum Gate { GATE_ALWAYS = 0, GATE_CHECK = 1, GATE_NOCHECK = 2 };
+
+// Precision-ladder phase in which a pass runs (independent of the gate).
+enum Phase {
+    PHASE_ANY = 0,
+    PHASE_FP32 = 1,      // runs while ctl->fp32_phase is set
+    PHASE_FP64 = 2,      // runs once ctl->fp32_phase is cleared
 };
 
 // Device-resident solver state. All fields written by device code are read by
@@ -135,7 +146,8 @@ struct Ctl {
     int error;                  // device-side error code (bounded waits etc.)
     int fp32_phase;             // precision ladder: FP32-exponent iterations still active
     double ladder_switch;       // ... until a check's L1 residual falls to this
-    double ladder_prev;         // the previous check's L1 residual (stall test)
+    double ladder_prev;         // the lowest check residual of the FP32 phase (stall test)
+    int ladder_bad;             // checks since that lowest residual
     long long loops;            // WHILE-body executions (independent loop bound)
 };
 
@@ -167,6 +179,7 @@ struct PassParams {
     int fp32;                   // 1 (with use_ref, p = 2, d <= 3): its exponent in FP32 (FORM_FP32)
     // gating and control
     int gate;
+    int phase;                  // Phase
     int finish;
     Ctl *ctl;
     // split-column scratch
@@ -539,9 +552,7 @@ static __device__ __noinline__ void run_finish(const PassParams &P, const double
             // precision ladder: FP64 passes from here once the residual is near
             // the tolerance, or once the FP32-exponent iteration stops gaining
             // (its rounding floor lies above the tolerance)
-            if (c->fp32_phase && (l1 <= c->ladder_switch || l1 >= LADDER_STALL * c->ladder_prev))
-                c->fp32_phase = 0;
-            c->ladder_prev = l1;
+            ladder_check(c->fp32_phase, c->ladder_prev, c->ladder_bad, l1, c->ladder_switch);
             put_log(c, (double)c->iter, l1, tot[1], nan(""), c->dualval + tot[2]);
             if (l1 <= c->epsilon / 6.0) { c->stop = 1; c->stop_reason = 1; }
             else {
@@ -590,6 +601,8 @@ static __device__ __noinline__ void run_finish(const PassParams &P, const double
             c->primal = primal;
             c->dual = dual;
             c->residual = c->sum_res_c;
+            // precision ladder, as in FIN_SK_CHECK, on the FP64 marginal residual
+            ladder_check(c->fp32_phase, c->ladder_prev, c->ladder_bad, c->sum_res_c, c->ladder_switch);
             c->objective = c->sum_cost;
             put_log(c, (double)(c->iter + 1), c->sum_res_c, c->sum_cost, primal, dual);
             const bool gap_ok = c->marginal_only ? true : (primal - dual < c->epsilon / 6.0);
@@ -1325,8 +1338,8 @@ __global__ void __launch_bounds__(TPB, (R > RPT_MID) ? 3 : 4)
         if (ctl->stop) return;
         if (P.gate == GATE_CHECK && !ctl->do_check) return;
         if (P.gate == GATE_NOCHECK && ctl->do_check) return;
-        if (P.gate == GATE_FP32 && !ctl->fp32_phase) return;
-        if (P.gate == GATE_FP64 && ctl->fp32_phase) return;
+        if (P.phase == PHASE_FP32 && !ctl->fp32_phase) return;
+        if (P.phase == PHASE_FP64 && ctl->fp32_phase) return;
     }
     double alpha = 0.0, beta = 0.0;
     if (ACC == ACC_LSE) resolve_coefs(P, alpha, beta);

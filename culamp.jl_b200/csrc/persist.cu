@@ -556,9 +556,11 @@ __global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_consta
     double residual = 0.0, objective = 0.0;
     // precision ladder (p = 2): FP32-exponent row and column passes while the
     // phase lasts; it ends, the same way in every CTA, at the first check whose
-    // FP64 residual is within ctl->ladder_switch or not below the previous one
-    bool fp32_phase = (PM == P_SQ) && ctl->fp32_phase;
+    // FP64 residual is within ctl->ladder_switch or has not improved for
+    // LADDER_PATIENCE checks
+    int fp32_phase = (PM == P_SQ && ctl->fp32_phase) ? 1 : 0;
     double ladder_prev = ctl->ladder_prev;
+    int ladder_bad = ctl->ladder_bad;
     const double ladder_switch = ctl->ladder_switch;
     for (;;) {
         if constexpr (PM == P_SQ) {
@@ -620,8 +622,7 @@ __global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_consta
         checked = true;
         residual = s_tot[1];
         objective = s_tot[2];
-        if (fp32_phase && (residual <= ladder_switch || residual >= LADDER_STALL * ladder_prev)) fp32_phase = false;
-        ladder_prev = residual;
+        ladder_check(fp32_phase, ladder_prev, ladder_bad, residual, ladder_switch);
         if (s_stop != 1) num_iter += 1;
         if (s_stop) { stop_reason = s_stop; break; }
     }
@@ -639,8 +640,9 @@ __global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_consta
     ctl->stop = 1;
     ctl->stop_reason = stop_reason;
     ctl->pending_stop = (stop_reason >= 2) ? stop_reason : 0;
-    ctl->fp32_phase = fp32_phase ? 1 : 0;
+    ctl->fp32_phase = fp32_phase;
     ctl->ladder_prev = ladder_prev;
+    ctl->ladder_bad = ladder_bad;
     if (checked) {
         ctl->residual = residual;
         ctl->objective = objective;

@@ -506,8 +506,8 @@ SkPlan make_sk_plan(culamp_handle h, int n, int m, int d, double p, uint32_t fla
             pl.k1f = pl.k1;
             pl.k2f = pl.k2;
             pl.k1f.fp32 = pl.k2f.fp32 = 1;
-            pl.k1f.gate = pl.k2f.gate = GATE_FP32;
-            pl.k1.gate = pl.k2.gate = GATE_FP64;
+            pl.k1f.phase = pl.k2f.phase = PHASE_FP32;
+            pl.k1.phase = pl.k2.phase = PHASE_FP64;
         }
     }
     pl.s_rows = pass_shape(n, m, d, ACC_LSE, h->sm_count);
@@ -853,13 +853,15 @@ namespace {
 
 struct LampPlan {
     PassParams k1, k2, k2m, kd, k3, k4;
+    PassParams k1f, k2f, k3f, k4f;   // precision ladder: FP32-exponent copies of k1 k2 k3 k4
+    bool ladder = false;
     int pm;
     bool dual_min;
     LaunchShape s_rows, s_cols, s_rows_min, s_cols_mom;
 };
 
 LampPlan make_lamp_plan(culamp_handle h, int n, int m, int d, double p, double winf, double eta,
-                        const culamp_args *args) {
+                        const culamp_args *args, uint32_t flags, bool checks) {
     Solver &S = *h->solver;
     Ctl *ctl = S.ctl.as<Ctl>();
     LampPlan pl;
@@ -939,6 +941,22 @@ LampPlan make_lamp_plan(culamp_handle h, int n, int m, int d, double p, double w
     pl.k4.gate = GATE_ALWAYS;
     pl.k4.lamp_step = LAMP_B;
     pl.k4.finish = FIN_LAMP_B;
+    // precision ladder (as for Sinkhorn): FP32-exponent logZ and column passes
+    // until a check's FP64 marginal residual is within 32x of the tolerance or
+    // stops falling. It needs the checks (verbose or CHECK_ALWAYS) and a
+    // tolerance; the check passes (cost moment, dual) stay FP64.
+    if (fp32_form_applies(S, d, pl.pm) && checks && args->epsilon > 0.0 && !(flags & CULAMP_FLAG_FORM_FP64) &&
+        ((flags & CULAMP_FLAG_LADDER) || (double)n * (double)m >= LADDER_AUTO_PAIRS)) {
+        pl.ladder = true;
+        PassParams *fp[4] = {&pl.k1f, &pl.k2f, &pl.k3f, &pl.k4f};
+        PassParams *dp[4] = {&pl.k1, &pl.k2, &pl.k3, &pl.k4};
+        for (int q = 0; q < 4; ++q) {
+            *fp[q] = *dp[q];
+            fp[q]->fp32 = 1;
+            fp[q]->phase = PHASE_FP32;
+            dp[q]->phase = PHASE_FP64;
+        }
+    }
     pl.s_rows = pass_shape(n, m, d, ACC_LSE, h->sm_count);
     pl.s_cols = pass_shape(m, n, d, ACC_LSE, h->sm_count);
     pl.s_rows_min = pass_shape(n, m, d, ACC_MIN, h->sm_count);
@@ -999,19 +1017,27 @@ extern "C" int culamp_lamp(culamp_handle h, const double *x, const double *y, in
     hc0.s_t = 1.0;
     hc0.tau_p = 1.0;   // hard-coded in the reference (MirrorProxKernel.jl:1073)
     hc0.hr = eta * sum_rlogr;
+    LampPlan pl = make_lamp_plan(h, (int)n, (int)m, d, p, winf, eta, args, flags, hc0.check_enabled != 0);
+    hc0.fp32_phase = pl.ladder ? 1 : 0;
+    hc0.ladder_switch = 32.0 * args->epsilon / 6.0;
+    hc0.ladder_prev = INFINITY;
     hc0.log = S.logbuf.as<culamp_log_row>();
     hc0.log_cap = log ? log_cap : 0;
     CUDA_TRY(h, cudaMemcpyAsync(S.ctl.ptr, &hc0, sizeof(Ctl), cudaMemcpyHostToDevice, st));
     set_start_kernel<<<1, 1, 0, st>>>(S.ctl.as<Ctl>());
-    LampPlan pl = make_lamp_plan(h, (int)n, (int)m, d, p, winf, eta, args);
     auto body = [&](cudaStream_t cs) -> cudaError_t {
-        cudaError_t e = launch_pass(pl.k1, pl.pm, ACC_LSE, pl.s_rows, S.scr, cs);
+        cudaError_t e = cudaSuccess;
+        if (pl.ladder) e = launch_pass(pl.k1f, pl.pm, ACC_LSE, pl.s_rows, S.scr, cs);
+        if (e == cudaSuccess) e = launch_pass(pl.k1, pl.pm, ACC_LSE, pl.s_rows, S.scr, cs);
+        if (e == cudaSuccess && pl.ladder) e = launch_pass(pl.k2f, pl.pm, ACC_LSE, pl.s_cols, S.scr, cs);
         if (e == cudaSuccess) e = launch_pass(pl.k2, pl.pm, ACC_LSE, pl.s_cols, S.scr, cs);
         if (e == cudaSuccess) e = launch_pass(pl.k2m, pl.pm, ACC_LSE, pl.s_cols_mom, S.scr, cs);
         if (e == cudaSuccess)
             e = launch_pass(pl.kd, pl.pm, pl.dual_min ? ACC_MIN : ACC_LSE,
                             pl.dual_min ? pl.s_rows_min : pl.s_rows, S.scr, cs);
+        if (e == cudaSuccess && pl.ladder) e = launch_pass(pl.k3f, pl.pm, ACC_LSE, pl.s_rows, S.scr, cs);
         if (e == cudaSuccess) e = launch_pass(pl.k3, pl.pm, ACC_LSE, pl.s_rows, S.scr, cs);
+        if (e == cudaSuccess && pl.ladder) e = launch_pass(pl.k4f, pl.pm, ACC_LSE, pl.s_cols, S.scr, cs);
         if (e == cudaSuccess) e = launch_pass(pl.k4, pl.pm, ACC_LSE, pl.s_cols, S.scr, cs);
         return e;
     };
@@ -1027,6 +1053,7 @@ extern "C" int culamp_lamp(culamp_handle h, const double *x, const double *y, in
     } else {
         GraphKey key;
         key.kind = KIND_LAMP;
+        key.form = pl.ladder ? 2 : 0;
         key.n = (int)n; key.m = (int)m; key.d = d;
         key.pm_iter = pl.pm;
         key.pm_resid = pl.dual_min ? 1 : 0;
@@ -1055,6 +1082,7 @@ extern "C" int culamp_lamp(culamp_handle h, const double *x, const double *y, in
         Ctl *pc = h->pass_ctl.as<Ctl>();
         PassParams a = pl.k1;
         a.ctl = pc;
+        a.phase = PHASE_ANY;
         a.coef_mode = COEF_FIXED;
         const double c1 = hc.s_t / (2.0 * winf), invreg = 1.0 / hc.eta_t;
         a.alpha = -c1 * invreg;
@@ -1063,6 +1091,7 @@ extern "C" int culamp_lamp(culamp_handle h, const double *x, const double *y, in
         CUDA_TRY(h, launch_pass(a, pl.pm, ACC_LSE, pl.s_rows, S.scr, st));
         PassParams b = pl.k2;
         b.ctl = pc;
+        b.phase = PHASE_ANY;
         b.coef_mode = COEF_FIXED;
         b.alpha = a.alpha;
         b.beta = a.beta;

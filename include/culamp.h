@@ -57,15 +57,18 @@ extern "C" {
 #define CULAMP_FLAG_FORM_FP32    128u  /* Sinkhorn, p = 2, d <= 3: the chosen form's engine with the
                                           exponent formed in FP32 (same tiling, reference,
                                           graph loop; ~1e-4 relative per term)               */
-#define CULAMP_FLAG_LADDER       256u  /* Sinkhorn, p = 2, d <= 3: FP32-exponent iterations until
-                                          a check's L1 residual falls to 32 x epsilon/6 or
-                                          stops falling (not below the previous check's),
-                                          then the FP64-exponent form to the tolerance. The
-                                          check passes are FP64 in every form.              */
-#define CULAMP_FLAG_FORM_FP64    512u  /* Sinkhorn: FP64-exponent passes throughout. Without it
-                                          (and without FORM_FP32) solves of n m >= 16384^2
-                                          pairs with p = 2 (or the p = Inf quirk) and d <= 3
-                                          take the precision ladder.                        */
+#define CULAMP_FLAG_LADDER       256u  /* Sinkhorn and LAMP, p = 2, d <= 3: FP32-exponent passes
+                                          until a check's FP64 L1 residual falls to
+                                          32 x epsilon/6 or stops falling (no new lowest
+                                          residual in 3 checks), then the FP64-exponent form
+                                          to the tolerance. The check passes are FP64 in every
+                                          form. LAMP needs its checks (verbose or
+                                          CHECK_ALWAYS) and epsilon > 0.                    */
+#define CULAMP_FLAG_FORM_FP64    512u  /* Sinkhorn / LAMP: FP64-exponent passes throughout.
+                                          Without it (and without FORM_FP32) solves of
+                                          n m >= 16384^2 pairs with p = 2 (Sinkhorn: or the
+                                          p = Inf quirk) and d <= 3 take the precision ladder
+                                          (LAMP: when it checks and epsilon > 0).           */
 #define CULAMP_FLAG_NO_PERSIST  1024u  /* Sinkhorn: one launch per pass (CUDA graph) instead of the
                                           whole loop in one persistent launch, which small
                                           problems (n, m <= 8192, d <= 3, p = 1, 2 or Inf)

@@ -179,3 +179,47 @@ def test_default_form_takes_the_ladder_above_16384_squared():
         assert res.stopped == 1
         rl, cl = cb.marginal_error_fp64(x, y, r, c, res.phi, res.psi, 1e-3, res.winf, 2.0)
         assert rl <= 1e-6 and cl <= 1e-6
+
+
+def test_lamp_ladder_reaches_tolerance_certified_in_fp64(dev_inst):
+    """LAMP (MirrorProxKernel.jl:1019-1132) with the precision ladder: the
+    logZ and column passes in FP32 exponents until a check's FP64 marginal
+    residual is within 32x of the tolerance; the checks themselves (cost
+    moment, dual value) stay FP64, so the stop is FP64-decided. The plan's
+    column marginal, recomputed in FP64 from the returned Sinkhorn-form
+    potentials (phi = log r - logZ, psi = -nu / eta_t), meets the tolerance."""
+    import culamp_b200 as cb
+    x, y, r, c = dev_inst
+    a = cb.EOTArgs(eta_p=1e-3, epsilon=6e-6, itermax=100_000, verbose=False, B=1.1)
+    fl = cb.FLAG_CHECK_ALWAYS | cb.FLAG_MARGINAL_ONLY
+    ref = cb.solve_lamp(x, y, r, c, a, 10, 2.0, flags=fl)
+    lad = cb.solve_lamp(x, y, r, c, a, 10, 2.0, flags=fl | cb.FLAG_LADDER)
+    print(f"LAMP ladder: {lad.iterations} iterations ({ref.iterations} FP64), {lad.elapsed_ms:.2f} ms "
+          f"({ref.elapsed_ms:.2f} ms FP64)")
+    assert ref.stopped == 1 and lad.stopped == 1
+    assert lad.residual <= 1e-6
+    assert abs(lad.iterations - ref.iterations) <= 0.1 * ref.iterations + 20
+    # Sinkhorn form of the LAMP plan: psi = -nu / eta_t, cost scale s / (2 W eta_t)
+    rl, cl = cb.marginal_error_fp64(x, y, r, c, lad.phi, -lad.nu / lad.eta_t, 1.0,
+                                    2.0 * lad.winf * lad.eta_t / lad.s_t, 2.0)
+    assert cl <= 1.5e-6 and rl <= 1e-6
+    # the FP32 phase takes LAMP along another path to the tolerance (its
+    # averaged potential is pinned only as far as the marginal test demands);
+    # the transport cost of the returned plan agrees with the FP64 form's
+    assert lad.objective == pytest.approx(ref.objective, rel=1e-5)
+
+
+def test_lamp_ladder_needs_checks(dev_inst):
+    """Without checks (verbose off, no CHECK_ALWAYS) LAMP cannot leave the FP32
+    phase, so the ladder flag leaves it in the FP64 form (the same passes; the
+    fixed-reference hints left in the workspace by the previous solve may route
+    a few rows through the online loop, so agreement is to FP32-sum rounding,
+    far below the FP32-exponent form's ~1e-4)."""
+    import culamp_b200 as cb
+    x, y, r, c = dev_inst
+    a = cb.EOTArgs(eta_p=1e-3, epsilon=6e-6, itermax=40, verbose=False, B=1.1)
+    ref = cb.solve_lamp(x, y, r, c, a, 10, 2.0)
+    lad = cb.solve_lamp(x, y, r, c, a, 10, 2.0, flags=cb.FLAG_LADDER)
+    assert ref.iterations == lad.iterations
+    want = _np(ref.nu)
+    np.testing.assert_allclose(_np(lad.nu), want, rtol=0, atol=1e-7 * max(1.0, np.abs(want).max()))
