@@ -64,11 +64,11 @@ extern "C" {
                                           to the tolerance. The check passes are FP64 in every
                                           form. LAMP needs its checks (verbose or
                                           CHECK_ALWAYS) and epsilon > 0.                    */
-#define CULAMP_FLAG_FORM_FP64    512u  /* Sinkhorn / LAMP: FP64-exponent passes throughout.
-                                          Without it (and without FORM_FP32) solves of
-                                          n m >= 16384^2 pairs with p = 2 (Sinkhorn: or the
-                                          p = Inf quirk) and d <= 3 take the precision ladder
-                                          (LAMP: when it checks and epsilon > 0).           */
+#define CULAMP_FLAG_FORM_FP64    512u  /* Sinkhorn: FP64-exponent passes throughout. Without
+                                          it (and without FORM_FP32) Sinkhorn solves of
+                                          n m >= 16384^2 pairs with p = 2 (or the p = Inf
+                                          quirk) and d <= 3 take the precision ladder. LAMP
+                                          takes the ladder only with FLAG_LADDER.           */
 #define CULAMP_FLAG_NO_PERSIST  1024u  /* Sinkhorn: one launch per pass (CUDA graph) instead of the
                                           whole loop in one persistent launch, which small
                                           problems (n, m <= 8192, d <= 3, p = 1, 2 or Inf)

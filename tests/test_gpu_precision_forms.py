@@ -203,10 +203,11 @@ def test_lamp_ladder_reaches_tolerance_certified_in_fp64(dev_inst):
     rl, cl = cb.marginal_error_fp64(x, y, r, c, lad.phi, -lad.nu / lad.eta_t, 1.0,
                                     2.0 * lad.winf * lad.eta_t / lad.s_t, 2.0)
     assert cl <= 1.5e-6 and rl <= 1e-6
-    # the FP32 phase takes LAMP along another path to the tolerance (its
-    # averaged potential is pinned only as far as the marginal test demands);
-    # the transport cost of the returned plan agrees with the FP64 form's
-    assert lad.objective == pytest.approx(ref.objective, rel=1e-5)
+    # the FP32 phase moves the iteration LAMP stops at, and with it eta_t (a
+    # function of the iteration count) and the returned plan's entropy: the
+    # transport cost agrees to ~1e-3, not to the FP64 form's 1e-5 -- which is
+    # why the LAMP ladder is opt-in
+    assert lad.objective == pytest.approx(ref.objective, rel=3e-3)
 
 
 def test_lamp_ladder_needs_checks(dev_inst):
