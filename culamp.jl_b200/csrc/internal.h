@@ -158,6 +158,22 @@ cudaError_t launch_sk_persist(const double *X, const double *Y, const double *r,
                               double *phi, double *psi, int n, int m, int d, int pm, double pexp,
                               Ctl *ctl, void *scratch, int grid, cudaStream_t st);
 
+// LAMP's loop (MirrorProxKernel.jl:1019-1132) in one persistent launch, same
+// problem sizes, eta_p > 0. Completes the control block like the graph loop.
+struct LampPersistArgs {
+    const double *X, *Y, *r, *c;
+    double *nu, *nub, *theta, *thetab;
+    const double *eta_mu;
+    double *logz, *aux;
+    int n, m, d, pm;
+    double pexp, eta_mu_exp, minv, maxv;
+    Ctl *ctl;
+    void *scratch;             // lamp_persist_scratch_bytes(grid)
+};
+int lamp_persist_grid(int sm_count, int d, int pm);
+size_t lamp_persist_scratch_bytes(int grid);
+cudaError_t launch_lamp_persist(const LampPersistArgs &a, int grid, cudaStream_t st);
+
 }  // namespace culamp_host
 
 // The opaque handle.

@@ -188,11 +188,11 @@ __device__ __forceinline__ float fr_term(double dv) {
 }
 
 // Exact FP64 online log-sum-exp of row o over all columns, by one warp (the
-// recompute of a row whose fixed-reference sum left the window). Every lane
-// returns the result.
+// recompute of a row whose fixed-reference sum left the window): terms
+// alpha C_oj + beta colpot_j, natural-log units. Every lane returns the result.
 template <int PM, int D>
 __device__ void row_lse_exact(const double *rows, int o, const double *cols, int nc, const double *colpot,
-                              double alpha, double inv_winf, double pexp, double &L, double &Ec) {
+                              double beta, double alpha, double inv_winf, double pexp, double &L, double &Ec) {
     const int lane = threadIdx.x & 31;
     double xv[D];
 #pragma unroll
@@ -203,7 +203,7 @@ __device__ void row_lse_exact(const double *rows, int o, const double *cols, int
 #pragma unroll
         for (int k = 0; k < D; ++k) yv[k] = cols[(size_t)j * D + k];
         const double cc = pair_cost_direct<PM>(xv, yv, D, pexp);
-        const double t = fma(alpha, cc, __ldcg(colpot + j));
+        const double t = fma(alpha, cc, beta * __ldcg(colpot + j));
         const double cn = cc * inv_winf;
         if (t == -INFINITY) continue;
         if (t > M) {
@@ -273,19 +273,16 @@ __device__ void cache_side(const Side &s, SideRows &R, const double (&ctr)[D], d
     }
 }
 
-enum HalfMode { HM_ROW = 0, HM_CHECK = 1 };
-
 // One half-step over this CTA's rows of side s (cached in R) against the
-// columns `cols` (nc points, potential colpot), in groups of PRG rows; warp 0
-// finishes each group (lane r = row r). HM_ROW: the row update of
-// warp_logsumexp_ct_fused! (EPI_SK_ROW): pot = log(marg) - L into R and s.pot,
-// K refreshed; part[0] = sum marg . pot. HM_CHECK: the row residual of
-// residual_opt! (EPI_SK_RESID): part = {sum |marg - mass|, sum mass E[C],
-// sum marg . pot}. part is valid in thread 0, in a fixed summation order.
-template <int PM, int D, bool MOM, int CB, bool F32 = false>
+// columns `cols` (nc points, potential colpot entering with coefficient cb,
+// log2 units), in groups of PRG rows; warp 0 finishes each group (lane r = row
+// r) with the row's natural-log LSE L (and with MOM its softmax-weighted mean
+// cost E) handed to the epilogue `epi`, whose four contributions per row are
+// summed into part (valid in thread 0, in a fixed summation order).
+template <int PM, int D, bool MOM, int CB, bool F32, class EPI, class SH>
 __device__ void pass_rows(const Side &s, SideRows &R, const double *cols, int nc, const double *colpot,
-                          const double (&ctr)[D], double a2, double inv_winf, double pexp, int mode,
-                          PShared &sh, double (&part)[3]) {
+                          double cb, const double (&ctr)[D], double a2, double inv_winf, double pexp,
+                          const EPI &epi, SH &sh, double (&part)[4]) {
     constexpr bool SQ = (PM == P_SQ);
     // window exponent: the row update's LSE may move well above its reference
     // (FR_C0 leaves 46 above); the check's hardly moves, and its cost moment
@@ -297,7 +294,7 @@ __device__ void pass_rows(const Side &s, SideRows &R, const double *cols, int nc
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int lo = rows_lo(s.n), cnt = rows_hi(s.n) - lo;
     const float invw_f = (float)inv_winf;
-    part[0] = part[1] = part[2] = 0.0;
+    part[0] = part[1] = part[2] = part[3] = 0.0;
     for (int g0 = 0; g0 < cnt; g0 += PRG) {
         const int nrows = min(PRG, cnt - g0);
         unsigned long long acc[NP], mo[MOM ? NP : 1];
@@ -325,7 +322,7 @@ __device__ void pass_rows(const Side &s, SideRows &R, const double *cols, int nc
                             s2 = fma(yy, yy, s2);
                             yf[k] = (float)yy;
                         }
-                        g = (float)(LOG2E * __ldcg(colpot + j) + a2 * s2);
+                        g = (float)(cb * __ldcg(colpot + j) + a2 * s2);
                     }
                     gy[c] = pack_f32x2(g, g);
                     y0[c] = pack_f32x2(yf[0], yf[0]);
@@ -363,7 +360,7 @@ __device__ void pass_rows(const Side &s, SideRows &R, const double *cols, int nc
                         yy[k] = cols[(size_t)j * D + k] - ctr[k];
                         s2 = fma(yy[k], yy[k], s2);
                     }
-                    g = LOG2E * __ldcg(colpot + j);
+                    g = cb * __ldcg(colpot + j);
                     if (SQ) g += a2 * s2;
                 }
                 col[c] = make_double4(yy[0], yy[1], yy[2], g);
@@ -462,40 +459,52 @@ __device__ void pass_rows(const Side &s, SideRows &R, const double *cols, int nc
                 const int rr = __ffs(bad) - 1;
                 bad &= bad - 1u;
                 double Lx, Ex;
-                row_lse_exact<PM, D>(s.pts, lo + g0 + rr, cols, nc, colpot, a2 * LN2, inv_winf, pexp, Lx, Ex);
+                row_lse_exact<PM, D>(s.pts, lo + g0 + rr, cols, nc, colpot, cb * LN2, a2 * LN2, inv_winf, pexp,
+                                     Lx, Ex);
                 if (lane == rr) { L = Lx; E = Ex; }
             }
-            double c0 = 0.0, c1 = 0.0, c2 = 0.0;
-            if (valid) {
-                const int o = lo + il;
-                if (mode == HM_ROW) {
-                    const double v = R.logm[il] - L;
-                    s.pot[o] = v;
-                    R.pot[il] = v;
-                    const double M2 = L * LOG2E - R.H[il];
-                    R.M2[il] = M2;
-                    R.xr[il].w = FR_MAGIC - (M2 + 1.0);
-                    R.xf[il].w = (float)(-M2);
-                    c0 = R.marg[il] * v;
-                } else {
-                    const double f = R.pot[il];
-                    const double mass = exp(f + L);
-                    c0 = fabs(R.marg[il] - mass);
-                    c1 = mass * E;
-                    c2 = R.marg[il] * f;
-                }
-            }
+            double cv[4] = {0.0, 0.0, 0.0, 0.0};
+            if (valid) epi(s, R, il, lo + il, L, E, cv);
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                c0 += __shfl_down_sync(0xffffffffu, c0, off);
-                c1 += __shfl_down_sync(0xffffffffu, c1, off);
-                c2 += __shfl_down_sync(0xffffffffu, c2, off);
-            }
-            if (lane == 0) { part[0] += c0; part[1] += c1; part[2] += c2; }
+            for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+                for (int k = 0; k < EPI::kN; ++k) cv[k] += __shfl_down_sync(0xffffffffu, cv[k], off);
+            if (lane == 0)
+#pragma unroll
+                for (int k = 0; k < EPI::kN; ++k) part[k] += cv[k];
         }
         if (g0 + PRG < cnt) __syncthreads();
     }
 }
+
+// Sinkhorn row update of warp_logsumexp_ct_fused! (EPI_SK_ROW): pot = log(marg)
+// - L into the cache and s.pot, the row's next reference L; cv[0] = marg . pot.
+struct EpiSkRow {
+    static constexpr int kN = 1;   // contributions per row
+    __device__ void operator()(const Side &s, SideRows &R, int il, int o, double L, double, double (&cv)[4]) const {
+        const double v = R.logm[il] - L;
+        s.pot[o] = v;
+        R.pot[il] = v;
+        const double M2 = L * LOG2E - R.H[il];
+        R.M2[il] = M2;
+        R.xr[il].w = FR_MAGIC - (M2 + 1.0);
+        R.xf[il].w = (float)(-M2);
+        cv[0] = R.marg[il] * v;
+    }
+};
+
+// Sinkhorn row residual of residual_opt! (EPI_SK_RESID): cv = {|marg - mass|,
+// mass E[C], marg . pot}.
+struct EpiSkResid {
+    static constexpr int kN = 3;
+    __device__ void operator()(const Side &, SideRows &R, int il, int, double L, double E, double (&cv)[4]) const {
+        const double f = R.pot[il];
+        const double mass = exp(f + L);
+        cv[0] = fabs(R.marg[il] - mass);
+        cv[1] = mass * E;
+        cv[2] = R.marg[il] * f;
+    }
+};
 
 // Sum over CTAs of slot k of the per-CTA partials, in CTA order (the same
 // value in every CTA).
@@ -505,23 +514,30 @@ __device__ __forceinline__ double cta_total(const double *blk, int k) {
     return s;
 }
 
-// The four slot totals over CTAs by one warp: lane l sums CTAs l, l + 32, ...
-// in order, then a fixed butterfly -- the same values in every CTA, since every
-// CTA runs the same steps on the same data. Valid in every lane.
-__device__ __forceinline__ void cta_totals4(const double *blk, double (&tot)[4]) {
+// The NS slot totals over CTAs ([G][NS] partials) by one warp: lane l sums
+// CTAs l, l + 32, ... in order, then a fixed butterfly -- the same values in
+// every CTA, since every CTA runs the same steps on the same data. Valid in
+// every lane.
+template <int NS>
+__device__ __forceinline__ void cta_totals(const double *blk, double (&tot)[NS]) {
+    static_assert(NS % 2 == 0, "slots are read in pairs");
     const int lane = threadIdx.x & 31;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) tot[k] = 0.0;
+    for (int k = 0; k < NS; ++k) tot[k] = 0.0;
     for (int b = lane; b < (int)gridDim.x; b += 32) {
-        const double2 v0 = __ldcg(reinterpret_cast<const double2 *>(blk + b * 4));
-        const double2 v1 = __ldcg(reinterpret_cast<const double2 *>(blk + b * 4 + 2));
-        tot[0] += v0.x; tot[1] += v0.y; tot[2] += v1.x; tot[3] += v1.y;
+#pragma unroll
+        for (int k = 0; k < NS; k += 2) {
+            const double2 v = __ldcg(reinterpret_cast<const double2 *>(blk + (size_t)b * NS + k));
+            tot[k] += v.x;
+            tot[k + 1] += v.y;
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
-        for (int k = 0; k < 4; ++k) tot[k] += __shfl_xor_sync(0xffffffffu, tot[k], o);
+        for (int k = 0; k < NS; ++k) tot[k] += __shfl_xor_sync(0xffffffffu, tot[k], o);
 }
+__device__ __forceinline__ void cta_totals4(const double *blk, double (&tot)[4]) { cta_totals<4>(blk, tot); }
 
 // The Sinkhorn loop (SinkhornKernel.jl:477-559): row update, column update,
 // and every `frequency` iterations the residual check, until the tolerance,
@@ -550,7 +566,7 @@ __global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_consta
     const double tol = ctl->epsilon / 6.0;
     const int b = blockIdx.x, tid = threadIdx.x;
     unsigned gen = 0;
-    double part[3];
+    double part[4];
     int stop_reason = 0;
     bool checked = false, failed = false;
     double residual = 0.0, objective = 0.0;
@@ -565,17 +581,19 @@ __global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_consta
     for (;;) {
         if constexpr (PM == P_SQ) {
             if (fp32_phase) {
-                pass_rows<PM, D, false, 4, true>(sx, sh.side[0], P.Y, P.m, P.psi, ctr, a2, inv_winf, P.pexp,
-                                                 HM_ROW, sh, part);
+                pass_rows<PM, D, false, 4, true>(sx, sh.side[0], P.Y, P.m, P.psi, LOG2E, ctr, a2, inv_winf,
+                                                 P.pexp, EpiSkRow{}, sh, part);
                 if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
-                pass_rows<PM, D, false, 4, true>(sy, sh.side[1], P.X, P.n, P.phi, ctr, a2, inv_winf, P.pexp,
-                                                 HM_ROW, sh, part);
+                pass_rows<PM, D, false, 4, true>(sy, sh.side[1], P.X, P.n, P.phi, LOG2E, ctr, a2, inv_winf,
+                                                 P.pexp, EpiSkRow{}, sh, part);
             }
         }
         if (!fp32_phase) {
-            pass_rows<PM, D, false, 4>(sx, sh.side[0], P.Y, P.m, P.psi, ctr, a2, inv_winf, P.pexp, HM_ROW, sh, part);
+            pass_rows<PM, D, false, 4, false>(sx, sh.side[0], P.Y, P.m, P.psi, LOG2E, ctr, a2, inv_winf, P.pexp,
+                                              EpiSkRow{}, sh, part);
             if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
-            pass_rows<PM, D, false, 4>(sy, sh.side[1], P.X, P.n, P.phi, ctr, a2, inv_winf, P.pexp, HM_ROW, sh, part);
+            pass_rows<PM, D, false, 4, false>(sy, sh.side[1], P.X, P.n, P.phi, LOG2E, ctr, a2, inv_winf, P.pexp,
+                                              EpiSkRow{}, sh, part);
         }
         if (tid == 0) {
             P.blk[b * 4 + 0] = part[0];
@@ -596,7 +614,8 @@ __global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_consta
             if (pending) { stop_reason = pending; break; }
             continue;
         }
-        pass_rows<PM, D, true, 2>(sx, sh.side[0], P.Y, P.m, P.psi, ctr, a2, inv_winf, P.pexp, HM_CHECK, sh, part);
+        pass_rows<PM, D, true, 2, false>(sx, sh.side[0], P.Y, P.m, P.psi, LOG2E, ctr, a2, inv_winf, P.pexp,
+                                             EpiSkResid{}, sh, part);
         if (tid == 0) {
             P.blk[b * 4 + 1] = part[0];
             P.blk[b * 4 + 2] = part[1];
@@ -647,6 +666,307 @@ __global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_consta
         ctl->residual = residual;
         ctl->objective = objective;
     }
+}
+
+
+// ---------------------------------------------------------------------------
+// LAMP (MirrorProxKernel.jl:1019-1132) in one persistent launch, small problems.
+//
+// An iteration is four passes, each a pass_rows over one side's rows:
+//   k1  logZ_i = LSE_j(alpha C_ij + beta nu_j) at (eta_t, s_t)          x rows
+//   k2  column residual at nu and the theta_bar / nu_bar step            y rows
+//       (with the cost moment on check iterations)
+//   kd  (check iterations) the dual pass LSE_j(alpha_d C_ij + beta_d theta_j)
+//       and the primal / dual / tolerance test                           x rows
+//   k3  logZ at nu_bar with (eta_next, s_next)                           x rows
+//   k4  column residual at nu_bar and the theta / nu step, the
+//       iteration bookkeeping                                            y rows
+// separated by grid barriers, as the pass engine's k1 k2 k2m kd k3 k4 with
+// FIN_LAMP_Z / A / DUAL / B. The coefficients change every pass (eta_t falls
+// ~1/t), so each pass first recomputes its rows' scaled coordinates and
+// fixed-reference offsets from the cached centred points and the row's
+// previous log-sum-exp (the dual pass keeps its own). The column state (nu,
+// nu_bar, theta, theta_bar, eta_mu) of a CTA's y rows lives in its shared
+// memory and is written through to HBM, where the x passes read it.
+
+struct LampParams {
+    const double *X, *Y, *r, *c;
+    double *nu, *nub, *theta, *thetab;   // column state (global copies)
+    const double *eta_mu;                 // per-column eta_mu_i
+    double *logz, *aux;                   // x rows: logZ and aux = log r - logZ
+    int n, m;
+    double pexp;
+    double eta_mu_exp, minv, maxv;
+    Ctl *ctl;
+    double *blk;                          // [G][LAMP_SLOTS] per-CTA partials
+    GridBar *bar;
+};
+constexpr int LAMP_SLOTS = 6;   // k1: sum r logZ; k2: |res - c|, cost, res nu, c theta; kd: sum r L
+
+struct LShared {
+    SideRows side[2];
+    double4 vv[2][PMAXR];      // centred point (v, |v|^2) of each cached row
+    double ref[2][PMAXR];      // natural-log LSE of the row's previous pass
+    double refd[PMAXR];        // x rows: of the previous dual pass
+    double nu[PMAXR], nub[PMAXR], th[PMAXR], thb[PMAXR], emu[PMAXR];   // y rows
+    float red[PWARPS][32];
+    float redm[PWARPS][32];
+    int flag;
+};
+
+// Rows of one side for a pass with exponent coefficient a2 (log2 units):
+// scaled coordinates, H = a2 |v|^2 (p = 2), M2 = ref log2(e) - H and the
+// fixed-reference offset K.
+template <int PM>
+__device__ void lamp_prep(SideRows &R, const double4 *vv, const double *ref, int cnt, double a2) {
+    constexpr bool SQ = (PM == P_SQ);
+    for (int i = threadIdx.x; i < PMAXR; i += PTPB) {
+        if (i >= cnt) {   // unused slots: finite junk, never finished
+            R.H[i] = 0.0;
+            R.M2[i] = 0.0;
+            R.xr[i] = make_double4(0.0, 0.0, 0.0, FR_MAGIC - 1.0);
+            continue;
+        }
+        const double4 v = vv[i];
+        const double H = SQ ? a2 * v.w : 0.0;
+        const double M2 = ref[i] * LOG2E - H;
+        R.H[i] = H;
+        R.M2[i] = M2;
+        R.xr[i] = SQ ? make_double4(-2.0 * a2 * v.x, -2.0 * a2 * v.y, -2.0 * a2 * v.z, FR_MAGIC - (M2 + 1.0))
+                     : make_double4(v.x, v.y, v.z, FR_MAGIC - (M2 + 1.0));
+    }
+    __syncthreads();
+}
+
+// k1 / k3 (EPI_LOGZ with FIN_LAMP_Z): logZ and aux = log r - logZ; cv[0] = r logZ.
+struct EpiLamZ {
+    static constexpr int kN = 1;
+    double *logz, *aux, *ref;
+    __device__ void operator()(const Side &, SideRows &R, int il, int o, double L, double, double (&cv)[4]) const {
+        logz[o] = L;
+        aux[o] = R.logm[il] - L;
+        ref[il] = L;
+        cv[0] = R.marg[il] * L;
+    }
+};
+
+// kd (EPI_LOGZ into the dual value): cv[0] = r L.
+struct EpiLamDual {
+    static constexpr int kN = 1;
+    double *refd;
+    __device__ void operator()(const Side &, SideRows &R, int il, int, double L, double, double (&cv)[4]) const {
+        refd[il] = L;
+        cv[0] = R.marg[il] * L;
+    }
+};
+
+// k2 / k4 (EPI_SPP_COL with the fused theta steps, MirrorProxKernel.jl:1104-1115):
+// res_j = exp(beta rowpot_j + L_j). STEP_A: theta_bar, nu_bar from theta, nu,
+// cv = {|res - c|, res E[C], res nu, c theta}; STEP_B: theta, nu from
+// theta_bar (adjusted into [minv, maxv]).
+template <bool STEP_A>
+struct EpiLamCol {
+    static constexpr int kN = STEP_A ? 4 : 0;
+    double beta, en, eta_mu_exp, minv, maxv;
+    double *g_nu, *g_nub, *g_th, *g_thb;
+    double *nu, *nub, *th, *thb, *emu, *ref;
+    __device__ void operator()(const Side &, SideRows &R, int il, int o, double L, double E, double (&cv)[4]) const {
+        const double cj = R.marg[il];
+        ref[il] = L;
+        if constexpr (STEP_A) {
+            const double rp = nu[il];
+            const double res = exp(beta * rp + L);
+            const double t0 = th[il];
+            cv[0] = fabs(res - cj);
+            cv[1] = res * E;
+            cv[2] = res * rp;
+            cv[3] = cj * t0;
+            const double tb = theta_step(t0, res, cj, emu[il], eta_mu_exp, 0, minv, maxv, 1.0);
+            const double nb = (1.0 - en) * rp + en * t0;
+            thb[il] = tb;
+            nub[il] = nb;
+            g_thb[o] = tb;
+            g_nub[o] = nb;
+        } else {
+            const double res = exp(beta * nub[il] + L);
+            const double t1 = theta_step(th[il], res, cj, emu[il], eta_mu_exp, 1, minv, maxv, 1.0);
+            const double n1 = (1.0 - en) * nu[il] + en * thb[il];
+            th[il] = t1;
+            nu[il] = n1;
+            g_th[o] = t1;
+            g_nu[o] = n1;
+        }
+    }
+};
+
+template <int PM, int D>
+__global__ void __launch_bounds__(PTPB, 1) lamp_persist_kernel(const __grid_constant__ LampParams P) {
+    __shared__ LShared sh;
+    __shared__ double s_tot[LAMP_SLOTS];
+    __shared__ double s_chk[4];     // residual, cost, primal, dual of the last check
+    __shared__ int s_stop;
+    constexpr bool SQ = (PM == P_SQ);
+    Ctl *ctl = P.ctl;
+    if (ctl->stop) return;
+    const double winf = ctl->winf, eta_l = ctl->eta_lamp, tau_p = ctl->tau_p, hr = ctl->hr;
+    const double tol = ctl->epsilon / 6.0;
+    const double inv_winf = 1.0 / winf;
+    const int check_enabled = ctl->check_enabled, marginal_only = ctl->marginal_only;
+    double ctr[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) ctr[k] = P.X[k];
+    const Side sx{P.X, P.r, P.aux, P.n};
+    const Side sy{P.Y, P.c, P.nu, P.m};
+    const int b = blockIdx.x, tid = threadIdx.x;
+    const int lx = rows_lo(P.n), cx = rows_hi(P.n) - lx;
+    const int ly = rows_lo(P.m), cy = rows_hi(P.m) - ly;
+    // row caches; the first pass of each kind has no reference yet (NaN: the
+    // window test fails and the rows take the exact loop)
+    for (int i = tid; i < PMAXR; i += PTPB) {
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const double *pts = side ? P.Y : P.X;
+            const int o = (side ? ly : lx) + i;
+            const bool ok = i < (side ? cy : cx);
+            double v[3] = {0.0, 0.0, 0.0}, h = 0.0;
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                v[k] = ok ? pts[(size_t)o * D + k] - ctr[k] : 0.0;
+                h = fma(v[k], v[k], h);
+            }
+            sh.vv[side][i] = make_double4(v[0], v[1], v[2], h);
+            sh.side[side].vf[i] = make_float4((float)v[0], (float)v[1], (float)v[2], 0.f);
+            const double mg = ok ? (side ? P.c[o] : P.r[o]) : 1.0;
+            sh.side[side].marg[i] = mg;
+            sh.side[side].logm[i] = log(mg);
+            sh.ref[side][i] = NAN;
+        }
+        sh.refd[i] = NAN;
+        const bool oky = i < cy;
+        const int oy = ly + i;
+        sh.nu[i] = oky ? P.nu[oy] : 0.0;
+        sh.nub[i] = oky ? P.nub[oy] : 0.0;
+        sh.th[i] = oky ? P.theta[oy] : 0.0;
+        sh.thb[i] = oky ? P.thetab[oy] : 0.0;
+        sh.emu[i] = oky ? P.eta_mu[oy] : 1.0;
+    }
+    if (tid < 4) s_chk[tid] = 0.0;
+    __syncthreads();
+    long long iter = ctl->iter;
+    const long long itermax = ctl->itermax, freq = ctl->frequency;
+    double eta_t = ctl->eta_t, s_t = ctl->s_t, eta_n = ctl->eta_next, s_n = ctl->s_next;
+    int do_check = ctl->do_check;
+    unsigned gen = 0;
+    double part[4];
+    int stop_reason = 0;
+    bool failed = false, checked = false;
+    for (;;) {
+        // k1: logZ at (nu, eta_t, s_t)
+        const double a2c = -s_t / (2.0 * winf * eta_t) * LOG2E;
+        const double bc = -1.0 / eta_t;
+        lamp_prep<PM>(sh.side[0], sh.vv[0], sh.ref[0], cx, a2c);
+        pass_rows<PM, D, false, 4, false>(sx, sh.side[0], P.Y, P.m, P.nu, bc * LOG2E, ctr, a2c, inv_winf, P.pexp,
+                                          EpiLamZ{P.logz, P.aux, sh.ref[0]}, sh, part);
+        if (tid == 0) P.blk[b * LAMP_SLOTS + 0] = part[0];
+        if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
+        // k2 (k2m on check iterations): column residual at nu, theta_bar / nu_bar step
+        lamp_next(eta_t, s_t, tau_p, eta_l, eta_n, s_n);
+        lamp_prep<PM>(sh.side[1], sh.vv[1], sh.ref[1], cy, a2c);
+        const EpiLamCol<true> ea{bc, eta_n, P.eta_mu_exp, P.minv, P.maxv, P.nu, P.nub, P.theta, P.thetab,
+                                 sh.nu, sh.nub, sh.th, sh.thb, sh.emu, sh.ref[1]};
+        if (do_check)
+            pass_rows<PM, D, true, 2, false>(sy, sh.side[1], P.X, P.n, P.aux, LOG2E, ctr, a2c, inv_winf, P.pexp,
+                                             ea, sh, part);
+        else
+            pass_rows<PM, D, false, 4, false>(sy, sh.side[1], P.X, P.n, P.aux, LOG2E, ctr, a2c, inv_winf, P.pexp,
+                                              ea, sh, part);
+        if (tid == 0)
+            for (int k = 0; k < 4; ++k) P.blk[b * LAMP_SLOTS + 1 + k] = part[k];
+        if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
+        if (do_check) {
+            // kd: the dual value at theta (eta_lamp, s = 1)
+            const double a2d = -1.0 / (2.0 * winf * eta_l) * LOG2E;
+            const double bd = -1.0 / eta_l;
+            lamp_prep<PM>(sh.side[0], sh.vv[0], sh.refd, cx, a2d);
+            pass_rows<PM, D, false, 4, false>(sx, sh.side[0], P.Y, P.m, P.theta, bd * LOG2E, ctr, a2d, inv_winf,
+                                              P.pexp, EpiLamDual{sh.refd}, sh, part);
+            if (tid == 0) P.blk[b * LAMP_SLOTS + 5] = part[0];
+            if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
+            // FIN_LAMP_A's sums and FIN_LAMP_DUAL (MirrorProxKernel.jl:1084-1100),
+            // the same in every CTA
+            if (tid < 32) {
+                double t6[LAMP_SLOTS];
+                cta_totals<LAMP_SLOTS>(P.blk, t6);
+                if (tid == 0)
+                    for (int k = 0; k < LAMP_SLOTS; ++k) s_tot[k] = t6[k];
+            }
+            if (tid == 0) {
+                const double sum_r_logz = s_tot[0], sum_res_c = s_tot[1], sum_cost = s_tot[2];
+                const double sum_res_nu = s_tot[3], sum_c_theta = s_tot[4];
+                const double q = eta_l / eta_t;
+                const double pr = sum_cost * (1.0 - q) - q * sum_res_nu + q * sum_r_logz + 2.0 * winf * sum_res_c;
+                const double du = -2.0 * eta_l * s_tot[5] - 2.0 * winf * sum_c_theta + 2.0 * hr;
+                if (b == 0) put_log(ctl, (double)(iter + 1), sum_res_c, sum_cost, pr, du);
+                const bool gap_ok = marginal_only ? true : (pr - du < tol);
+                s_stop = (gap_ok && sum_res_c < tol) ? 1 : 0;
+                s_chk[0] = sum_res_c; s_chk[1] = sum_cost; s_chk[2] = pr; s_chk[3] = du;
+            }
+            __syncthreads();
+            checked = true;
+            if (s_stop) { stop_reason = 1; break; }
+        }
+        // k3: logZ at (nu_bar, eta_next, s_next)
+        const double a2n = -s_n / (2.0 * winf * eta_n) * LOG2E;
+        const double bn = -1.0 / eta_n;
+        lamp_prep<PM>(sh.side[0], sh.vv[0], sh.ref[0], cx, a2n);
+        pass_rows<PM, D, false, 4, false>(sx, sh.side[0], P.Y, P.m, P.nub, bn * LOG2E, ctr, a2n, inv_winf, P.pexp,
+                                          EpiLamZ{P.logz, P.aux, sh.ref[0]}, sh, part);
+        if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
+        // k4: column residual at nu_bar, theta / nu step
+        lamp_prep<PM>(sh.side[1], sh.vv[1], sh.ref[1], cy, a2n);
+        const EpiLamCol<false> eb{bn, eta_n, P.eta_mu_exp, P.minv, P.maxv, P.nu, P.nub, P.theta, P.thetab,
+                                  sh.nu, sh.nub, sh.th, sh.thb, sh.emu, sh.ref[1]};
+        pass_rows<PM, D, false, 4, false>(sy, sh.side[1], P.X, P.n, P.aux, LOG2E, ctr, a2n, inv_winf, P.pexp,
+                                          eb, sh, part);
+        if (tid == 0 && b == 0) {
+            const bool late = (double)(globaltimer_ns() - ctl->t_start_ns) * 1e-9 > ctl->tmax_s;
+            atomicExch(&P.bar->tmax_hit, late ? 1u : 0u);
+        }
+        if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
+        // FIN_LAMP_B, the same in every CTA
+        eta_t = eta_n;
+        s_t = s_n;
+        iter += 1;
+        int pending = 0;
+        if (iter >= itermax) pending = 2;
+        else if (ld_acquire_u32(&P.bar->tmax_hit)) pending = 3;
+        do_check = check_enabled && (iter % freq) == 0;
+        if (pending) { stop_reason = pending; break; }
+    }
+    if (tid != 0) return;
+    if (failed) {
+        ctl->error = 1;
+        ctl->stop = 1;
+        return;
+    }
+    if (b != 0) return;
+    ctl->iter = iter;
+    ctl->num_iter = iter;
+    ctl->eta_t = eta_t;
+    ctl->s_t = s_t;
+    ctl->eta_next = eta_n;
+    ctl->s_next = s_n;
+    ctl->do_check = do_check;
+    ctl->stop = 1;
+    ctl->stop_reason = stop_reason;
+    ctl->pending_stop = (stop_reason >= 2) ? stop_reason : 0;
+    if (checked) {
+        ctl->residual = s_chk[0];
+        ctl->objective = s_chk[1];
+        ctl->primal = s_chk[2];
+        ctl->dual = s_chk[3];
+    }
+    (void)SQ;
 }
 
 }  // namespace culamp_dev
@@ -703,6 +1023,57 @@ int persist_grid(int sm_count, int d, int pm) {
         return 0;
     }
     return sm_count;   // one CTA per SM
+}
+
+namespace {
+
+using LampFn = void (*)(LampParams);
+
+LampFn lamp_fn(int d, int pm) {
+    if (pm == P_SQ) return d == 1 ? lamp_persist_kernel<P_SQ, 1> : d == 2 ? lamp_persist_kernel<P_SQ, 2> : lamp_persist_kernel<P_SQ, 3>;
+    if (pm == P_L1) return d == 1 ? lamp_persist_kernel<P_L1, 1> : d == 2 ? lamp_persist_kernel<P_L1, 2> : lamp_persist_kernel<P_L1, 3>;
+    return d == 1 ? lamp_persist_kernel<P_INF, 1> : d == 2 ? lamp_persist_kernel<P_INF, 2> : lamp_persist_kernel<P_INF, 3>;
+}
+
+}  // namespace
+
+int lamp_persist_grid(int sm_count, int d, int pm) {
+    int per_sm = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lamp_fn(d, pm), PTPB, 0);
+    if (e != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        return 0;
+    }
+    return sm_count;
+}
+
+size_t lamp_persist_scratch_bytes(int grid) {
+    return (size_t)grid * LAMP_SLOTS * sizeof(double) + sizeof(GridBar);
+}
+
+cudaError_t launch_lamp_persist(const LampPersistArgs &a, int grid, cudaStream_t st) {
+    LampParams P;
+    P.X = a.X; P.Y = a.Y; P.r = a.r; P.c = a.c;
+    P.nu = a.nu; P.nub = a.nub; P.theta = a.theta; P.thetab = a.thetab;
+    P.eta_mu = a.eta_mu;
+    P.logz = a.logz; P.aux = a.aux;
+    P.n = a.n; P.m = a.m; P.pexp = a.pexp;
+    P.eta_mu_exp = a.eta_mu_exp; P.minv = a.minv; P.maxv = a.maxv;
+    P.ctl = a.ctl;
+    P.blk = reinterpret_cast<double *>(a.scratch);
+    P.bar = reinterpret_cast<GridBar *>(P.blk + (size_t)grid * LAMP_SLOTS);
+    cudaError_t e = cudaMemsetAsync(P.bar, 0, sizeof(GridBar), st);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(PTPB);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, lamp_fn(a.d, a.pm), P);
 }
 
 cudaError_t launch_sk_persist(const double *X, const double *Y, const double *r, const double *c,

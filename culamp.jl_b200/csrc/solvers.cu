@@ -1043,8 +1043,35 @@ extern "C" int culamp_lamp(culamp_handle h, const double *x, const double *y, in
         if (e == cudaSuccess) e = launch_pass(pl.k4, pl.pm, ACC_LSE, pl.s_cols, S.scr, cs);
         return e;
     };
+    // small problems: the whole loop in one persistent cooperative launch
+    const bool lpersist = !(flags & (CULAMP_FLAG_NO_GRAPH | CULAMP_FLAG_NO_PERSIST)) && !pl.ladder &&
+                          !pl.dual_min && !S.feat_active && d <= MAXD_PACKED &&
+                          (pl.pm == P_L1 || pl.pm == P_SQ || pl.pm == P_INF);
+    int lgrid = lpersist ? lamp_persist_grid(h->sm_count, d, pl.pm) : 0;
+    if (lgrid > 0 && !persist_eligible((int)n, (int)m, d, pl.pm, pl.pm, lgrid)) lgrid = 0;
+    if (lgrid > 0) CUDA_TRY(h, S.pers.reserve(lamp_persist_scratch_bytes(lgrid)));
     CUDA_TRY(h, cudaEventRecord(S.ev0, st));
-    if (flags & CULAMP_FLAG_NO_GRAPH) {
+    bool lran = false;
+    if (lgrid > 0) {
+        LampPersistArgs la;
+        la.X = S.X.as<double>(); la.Y = S.Y.as<double>(); la.r = S.r.as<double>(); la.c = S.c.as<double>();
+        la.nu = S.nu.as<double>(); la.nub = S.nub.as<double>();
+        la.theta = S.theta.as<double>(); la.thetab = S.thetab.as<double>();
+        la.eta_mu = S.eta_mu.as<double>();
+        la.logz = S.logz.as<double>(); la.aux = S.aux.as<double>();
+        la.n = (int)n; la.m = (int)m; la.d = d; la.pm = pl.pm;
+        la.pexp = p;
+        la.eta_mu_exp = args->eta_mu;
+        la.minv = std::tanh(-args->B / 2.0);
+        la.maxv = std::tanh(args->B / 2.0);
+        la.ctl = S.ctl.as<Ctl>();
+        la.scratch = S.pers.ptr;
+        // a refused cooperative launch falls back to the graph loop
+        if (launch_lamp_persist(la, lgrid, st) == cudaSuccess) lran = true;
+        else cudaGetLastError();
+    }
+    if (lran) {
+    } else if (flags & CULAMP_FLAG_NO_GRAPH) {
         for (long long it = 0; it < args->itermax + 2; ++it) {
             CUDA_TRY(h, body(st));
             int stop = 0;

@@ -162,3 +162,76 @@ def test_ladder_in_the_persistent_loop(grid):
     scale = max(1.0, np.abs(_np(f64.phi)).max())
     assert np.abs((_np(lad.phi) - k1) - (_np(f64.phi) - k0)).max() <= 1e-5 * scale
     assert np.abs((_np(lad.psi) + k1) - (_np(f64.psi) + k0)).max() <= 1e-5 * scale
+
+
+# ----------------------------------------------------------------- LAMP
+
+def lamp_both(x, y, r, c, a, freq, p, flags=0):
+    import culamp_b200 as cb
+    per = cb.solve_lamp(x, y, r, c, a, freq, p, flags=flags)
+    ref = cb.solve_lamp(x, y, r, c, a, freq, p, flags=flags | cb.FLAG_NO_PERSIST)
+    return per, ref
+
+
+def lamp_same(per, ref):
+    """Counters, eta_t (a function of the iteration count: bit-exact), the
+    check rows; theta / nu to the FP32 term-sum rounding amplified by the
+    mirror step's 1 / eta_mu_j (~m), as for the sharded LAMP."""
+    assert per.iterations == ref.iterations and per.stopped == ref.stopped
+    assert per.eta_t == ref.eta_t and per.s_t == ref.s_t
+    assert len(per.log) == len(ref.log)
+    if per.log:
+        g = np.array([row[1:6] for row in per.log])
+        w = np.array([row[1:6] for row in ref.log])
+        assert np.array_equal(g[:, 0], w[:, 0])
+        np.testing.assert_allclose(g[:, 1], w[:, 1], rtol=1e-3, atol=2e-7)     # marginal residual
+        np.testing.assert_allclose(g[:, 2], w[:, 2], rtol=1e-5, atol=1e-7)      # cost
+        np.testing.assert_allclose(g[:, 3:5], w[:, 3:5], rtol=1e-4, atol=1e-6)  # primal, dual
+    np.testing.assert_allclose(_np(per.theta), _np(ref.theta), rtol=0, atol=5e-5)
+    np.testing.assert_allclose(_np(per.nu), _np(ref.nu), rtol=0, atol=5e-5)
+    assert per.objective == pytest.approx(ref.objective, rel=1e-5)
+
+
+@pytest.mark.parametrize("eta_p", [1e-3, 1e-4])
+@pytest.mark.parametrize("p", [1.0, 2.0, math.inf])
+def test_lamp_fixed_iterations_match_graph_loop(grid, p, eta_p):
+    import culamp_b200 as cb
+    a = cb.EOTArgs(eta_p=eta_p, epsilon=0.0, itermax=60, verbose=True, B=1.1)
+    per, ref = lamp_both(*grid, a, 10, p)
+    lamp_same(per, ref)
+
+
+@pytest.mark.parametrize("flags", ["full", "marginal"])
+def test_lamp_stops_where_the_graph_loop_stops(grid, flags):
+    import culamp_b200 as cb
+    fl = cb.FLAG_CHECK_ALWAYS | (cb.FLAG_MARGINAL_ONLY if flags == "marginal" else 0)
+    # the full rule's gap does not close to 1e-6 on this instance: both loops
+    # run to itermax there, with the same check rows
+    a = cb.EOTArgs(eta_p=1e-3, epsilon=6e-6, itermax=2000, verbose=False, B=1.1)
+    per, ref = lamp_both(*grid, a, 10, 2.0, fl)
+    print(f"4096 LAMP ({flags}): persistent {per.elapsed_ms:.2f} ms, graph loop {ref.elapsed_ms:.2f} ms, "
+          f"{per.iterations} iterations")
+    lamp_same(per, ref)
+
+
+@pytest.mark.parametrize("n,m,d", [(5, 7, 3), (1000, 3000, 3), (2500, 1200, 2), (8192, 8192, 3)])
+def test_lamp_ragged_shapes(n, m, d):
+    import torch
+    import culamp_b200 as cb
+    g = np.random.Generator(np.random.PCG64(n * 37 + m))
+    x = torch.as_tensor(g.uniform(0, 1, (n, d)), device="cuda")
+    y = torch.as_tensor(g.uniform(0, 1, (m, d)), device="cuda")
+    r = torch.as_tensor(g.uniform(0.5, 1.0, n), device="cuda")
+    c = torch.as_tensor(g.uniform(0.5, 1.0, m), device="cuda")
+    r, c = r / r.sum(), c / c.sum()
+    a = cb.EOTArgs(eta_p=5e-3, epsilon=0.0, itermax=25, verbose=True, B=1.1)
+    per, ref = lamp_both(x, y, r, c, a, 5, 2.0)
+    lamp_same(per, ref)
+
+
+def test_lamp_itermax_and_tmax(grid):
+    import culamp_b200 as cb
+    for kw in (dict(itermax=7), dict(itermax=1000, tmax=0.0)):
+        a = cb.EOTArgs(eta_p=1e-2, epsilon=0.0, verbose=True, B=1.1, **kw)
+        per, ref = lamp_both(*grid, a, 3, 2.0)
+        lamp_same(per, ref)
