@@ -20,8 +20,9 @@
 //     each row's fixed-reference offset in that cache.
 //   * Each term uses the fixed-reference exponent of the pass engine (DADD with
 //     FR_MAGIC, funnel-shifted mantissa, one MUFU ex2, exponent-field add,
-//     scaled by 2^FR_C0). A row whose sum leaves the window is recomputed by one
-//     warp with an FP64 online log-sum-exp (exact exp) over all columns.
+//     scaled by 2^FR_C0). Rows whose sums leave the window are shared out to
+//     the CTA's warps and recomputed without a reference (a max pass, then a
+//     sum pass of max-shifted terms).
 //   * Half-steps are separated by a grid barrier (one arrival counter and one
 //     generation word in global memory). Every wait on it is bounded: after
 //     PERSIST_WAIT_NS a waiting CTA sets the abort word and the control block's
@@ -135,6 +136,8 @@ struct PShared {
     SideRows side[2];          // 0: the x points (phi), 1: the y points (psi)
     float red[PWARPS][32];
     float redm[PWARPS][32];
+    double fl[32], fe[32];     // the group's rows recomputed by the fallback
+    unsigned bad;              // rows of the group outside the window
     int flag;
 };
 
@@ -187,56 +190,50 @@ __device__ __forceinline__ float fr_term(double dv) {
     }
 }
 
-// Exact FP64 online log-sum-exp of row o over all columns, by one warp (the
-// recompute of a row whose fixed-reference sum left the window): terms
-// alpha C_oj + beta colpot_j, natural-log units. Every lane returns the result.
-template <int PM, int D>
-__device__ void row_lse_exact(const double *rows, int o, const double *cols, int nc, const double *colpot,
-                              double beta, double alpha, double inv_winf, double pexp, double &L, double &Ec) {
+// Log-sum-exp of row o over all columns by one warp, without a reference: the
+// recompute of a row whose fixed-reference sum left the window. Terms
+// t_j = alpha C_oj + beta colpot_j (natural-log units) in FP64; first their
+// maximum M, then 2^((t_j - M) log2 e) on the MUFU pipe (the online loop's
+// term, |t_j - M| rounded to FP32) in Kahan-compensated FP32 sums per lane,
+// merged in FP64. With MOM also the cost moment. Every lane returns L, E.
+template <int PM, int D, bool MOM>
+__device__ void row_lse_twopass(const double *rows, int o, const double *cols, int nc, const double *colpot,
+                                double beta, double alpha, double inv_winf, double pexp, double &L, double &Ec) {
     const int lane = threadIdx.x & 31;
     double xv[D];
 #pragma unroll
     for (int k = 0; k < D; ++k) xv[k] = rows[(size_t)o * D + k];
-    double M = -INFINITY, S = 0.0, MO = 0.0;
+    double M = -INFINITY;
     for (int j = lane; j < nc; j += 32) {
         double yv[D];
 #pragma unroll
         for (int k = 0; k < D; ++k) yv[k] = cols[(size_t)j * D + k];
-        const double cc = pair_cost_direct<PM>(xv, yv, D, pexp);
-        const double t = fma(alpha, cc, beta * __ldcg(colpot + j));
-        const double cn = cc * inv_winf;
-        if (t == -INFINITY) continue;
-        if (t > M) {
-            const double f = exp(M - t);
-            S = S * f + 1.0;
-            MO = MO * f + cn;
-            M = t;
-        } else {
-            const double e = exp(t - M);
-            S += e;
-            MO = fma(e, cn, MO);
-        }
+        const double t = fma(alpha, pair_cost_direct<PM>(xv, yv, D, pexp), beta * __ldcg(colpot + j));
+        M = fmax(M, t);
     }
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        const double M2 = __shfl_xor_sync(0xffffffffu, M, off);
-        const double S2 = __shfl_xor_sync(0xffffffffu, S, off);
-        const double MO2 = __shfl_xor_sync(0xffffffffu, MO, off);
-        if (M2 == -INFINITY) continue;
-        if (M == -INFINITY) { M = M2; S = S2; MO = MO2; continue; }
-        if (M2 > M) {
-            const double f = exp(M - M2);
-            S = S * f + S2;
-            MO = MO * f + MO2;
-            M = M2;
-        } else {
-            const double f = exp(M2 - M);
-            S += S2 * f;
-            MO += MO2 * f;
+    for (int off = 16; off > 0; off >>= 1) M = fmax(M, __shfl_xor_sync(0xffffffffu, M, off));
+    float S = 0.f, Sc = 0.f, MO = 0.f, MOc = 0.f;
+    if (M > -INFINITY) {
+        for (int j = lane; j < nc; j += 32) {
+            double yv[D];
+#pragma unroll
+            for (int k = 0; k < D; ++k) yv[k] = cols[(size_t)j * D + k];
+            const double cc = pair_cost_direct<PM>(xv, yv, D, pexp);
+            const double t = fma(alpha, cc, beta * __ldcg(colpot + j));
+            const float e = ex2_approx((float)((t - M) * LOG2E));
+            kahan_add(S, Sc, e);
+            if (MOM) kahan_add(MO, MOc, e * (float)(cc * inv_winf));
         }
     }
-    L = M + log(S);
-    Ec = (S > 0.0) ? MO / S * (1.0 / inv_winf) : 0.0;
+    double Sd = (double)S - (double)Sc, MOd = (double)MO - (double)MOc;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        Sd += __shfl_xor_sync(0xffffffffu, Sd, off);
+        MOd += __shfl_xor_sync(0xffffffffu, MOd, off);
+    }
+    L = M + log(Sd);
+    Ec = (MOM && Sd > 0.0) ? MOd / Sd / inv_winf : 0.0;
 }
 
 // Kernel-entry set-up of this CTA's rows of one side.
@@ -434,9 +431,10 @@ __device__ void pass_rows(const Side &s, SideRows &R, const double *cols, int nc
             sh.redm[warp][lane] = a[0];
         }
         __syncthreads();
+        double L = 0.0, E = 0.0;
+        const bool valid = lane < nrows;
+        const int il = g0 + (valid ? lane : 0);
         if (warp == 0) {
-            const bool valid = lane < nrows;
-            const int il = g0 + (valid ? lane : 0);
             double S = 0.0, MOv = 0.0;
 #pragma unroll
             for (int w = 0; w < PWARPS; ++w) {
@@ -449,20 +447,30 @@ __device__ void pass_rows(const Side &s, SideRows &R, const double *cols, int nc
             // FP32 exponents: unscaled terms, the engine's 2^64 / FR32_LOW_MARGIN window
             const bool good = F32 ? (S > 0.0 && S <= 0x1p64 && log2(S) >= -FR32_LOW_MARGIN)
                                   : (S > 0.0 && S <= FR_SUM_MAX && log2(S) >= 32.0 + log2((double)nc));
-            double L = 0.0, E = 0.0;
             if (valid && good) {
                 L = LN2 * (R.H[il] + R.M2[il] + (log2(S) - (F32 ? 0.0 : (double)C0)));
                 E = MOM ? MOv / S / inv_winf : 0.0;
             }
-            unsigned bad = __ballot_sync(0xffffffffu, valid && !good);
-            while (bad) {
-                const int rr = __ffs(bad) - 1;
-                bad &= bad - 1u;
-                double Lx, Ex;
-                row_lse_exact<PM, D>(s.pts, lo + g0 + rr, cols, nc, colpot, cb * LN2, a2 * LN2, inv_winf, pexp,
-                                     Lx, Ex);
-                if (lane == rr) { L = Lx; E = Ex; }
+            const unsigned bad = __ballot_sync(0xffffffffu, valid && !good);
+            if (lane == 0) sh.bad = bad;
+        }
+        __syncthreads();
+        if (sh.bad) {
+            // rows outside the window (a reference far from the new LSE): the
+            // warps share them, each row by the two-pass loop of row_lse_twopass
+            for (int k = 0, seen = 0; k < 32; ++k) {
+                if (!((sh.bad >> k) & 1u)) continue;
+                if ((seen++ % PWARPS) == warp) {
+                    double Lx, Ex;
+                    row_lse_twopass<PM, D, MOM>(s.pts, lo + g0 + k, cols, nc, colpot, cb * LN2, a2 * LN2,
+                                                inv_winf, pexp, Lx, Ex);
+                    if (lane == 0) { sh.fl[k] = Lx; sh.fe[k] = Ex; }
+                }
             }
+            __syncthreads();
+            if (warp == 0 && ((sh.bad >> lane) & 1u)) { L = sh.fl[lane]; E = sh.fe[lane]; }
+        }
+        if (warp == 0) {
             double cv[4] = {0.0, 0.0, 0.0, 0.0};
             if (valid) epi(s, R, il, lo + il, L, E, cv);
 #pragma unroll
@@ -711,6 +719,8 @@ struct LShared {
     double nu[PMAXR], nub[PMAXR], th[PMAXR], thb[PMAXR], emu[PMAXR];   // y rows
     float red[PWARPS][32];
     float redm[PWARPS][32];
+    double fl[32], fe[32];     // the group's rows recomputed by the fallback
+    unsigned bad;              // rows of the group outside the window
     int flag;
 };
 
