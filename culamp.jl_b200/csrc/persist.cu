@@ -51,10 +51,13 @@ constexpr int PMAXR = 56;                  // rows per CTA and side (2 groups)
 constexpr unsigned long long PERSIST_WAIT_NS = 2000000000ull;
 
 struct GridBar {
-    unsigned long long count;   // arrivals since the launch (+ PERSIST_ABORT once a CTA gave up)
-    unsigned tmax_hit;          // CTA 0's clock decision for the current iteration
-    unsigned pad;
+    // arrivals since the launch in the low 44 bits; + PERSIST_LATE once CTA 0
+    // has found tmax passed, + PERSIST_ABORT once a CTA gave up waiting
+    unsigned long long count;
+    unsigned long long pad;
 };
+constexpr unsigned long long PERSIST_LATE = 1ull << 44;
+constexpr unsigned long long PERSIST_ARRIVALS = PERSIST_LATE - 1ull;
 constexpr unsigned long long PERSIST_ABORT = 1ull << 62;
 
 struct PersistParams {
@@ -68,11 +71,6 @@ struct PersistParams {
     GridBar *bar;              // zeroed before the launch
 };
 
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
     unsigned long long v;
     asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
@@ -88,19 +86,27 @@ __device__ __forceinline__ void red_release_add_u64(unsigned long long *p, unsig
 // polls the counter with acquire loads; bar.sync before the arrival and after
 // the wait extends both to the whole CTA. A CTA that gives up after
 // PERSIST_WAIT_NS adds PERSIST_ABORT, which every waiter sees at once.
+// The arrival can carry `extra` (CTA 0: PERSIST_LATE, its tmax decision);
+// `*s_late` then tells every CTA, from the same counter read, whether it was
+// added by the time the barrier completed -- CTA 0 adds it only at the barrier
+// that ends an iteration, and stops after it, so every CTA sees the same.
 // Returns false (in every thread of the CTA) when this CTA gave up or saw
 // another CTA give up.
-__device__ bool grid_sync(GridBar *gb, unsigned &gen, int *s_flag) {
+__device__ bool grid_sync(GridBar *gb, unsigned &gen, int *s_flag, unsigned long long extra = 0ull,
+                          int *s_late = nullptr) {
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        red_release_add_u64(&gb->count, 1ull);
+        red_release_add_u64(&gb->count, 1ull + extra);
         const unsigned long long target = (unsigned long long)(gen + 1u) * gridDim.x;
         unsigned long long t0 = 0;
         for (unsigned spins = 0;; ++spins) {
             const unsigned long long v = ld_acquire_u64(&gb->count);
             if (v >= PERSIST_ABORT) { ok = 0; break; }
-            if (v >= target) break;
+            if ((v & PERSIST_ARRIVALS) >= target) {
+                if (s_late) *s_late = (v & ~PERSIST_ARRIVALS) != 0ull;
+                break;
+            }
             if ((spins & 63u) == 63u) {
                 const unsigned long long t = globaltimer_ns();
                 if (t0 == 0) t0 = t;
@@ -139,6 +145,7 @@ struct PShared {
     double fl[32], fe[32];     // the group's rows recomputed by the fallback
     unsigned bad;              // rows of the group outside the window
     int flag;
+    int late;                  // tmax passed (CTA 0's decision, via the barrier)
 };
 
 // One side of the problem as the rows of a half-step.
@@ -292,6 +299,7 @@ __device__ void pass_rows(const Side &s, SideRows &R, const double *cols, int nc
     const int lo = rows_lo(s.n), cnt = rows_hi(s.n) - lo;
     const float invw_f = (float)inv_winf;
     part[0] = part[1] = part[2] = part[3] = 0.0;
+    const double low_floor = 32.0 + log2((double)nc);   // lower side of the window on log2(S)
     for (int g0 = 0; g0 < cnt; g0 += PRG) {
         const int nrows = min(PRG, cnt - g0);
         unsigned long long acc[NP], mo[MOM ? NP : 1];
@@ -443,10 +451,10 @@ __device__ void pass_rows(const Side &s, SideRows &R, const double *cols, int nc
             }
             // the window: no term clamped high (S <= 2^126 scaled), and the full
             // sum within C0 - 32 - log2(nc) below the reference (the engine's
-            // fr_low_margin), i.e. log2(S) >= 32 + log2(nc)
+            // fr_low_margin), i.e. log2(S) >= 32 + log2(nc) = low_floor
             // FP32 exponents: unscaled terms, the engine's 2^64 / FR32_LOW_MARGIN window
             const bool good = F32 ? (S > 0.0 && S <= 0x1p64 && log2(S) >= -FR32_LOW_MARGIN)
-                                  : (S > 0.0 && S <= FR_SUM_MAX && log2(S) >= 32.0 + log2((double)nc));
+                                  : (S > 0.0 && S <= FR_SUM_MAX && log2(S) >= low_floor);
             if (valid && good) {
                 L = LN2 * (R.H[il] + R.M2[il] + (log2(S) - (F32 ? 0.0 : (double)C0)));
                 E = MOM ? MOv / S / inv_winf : 0.0;
@@ -603,19 +611,17 @@ __global__ void __launch_bounds__(PTPB, 1) sk_persist_kernel(const __grid_consta
             pass_rows<PM, D, false, 4, false>(sy, sh.side[1], P.X, P.n, P.phi, LOG2E, ctr, a2, inv_winf, P.pexp,
                                               EpiSkRow{}, sh, part);
         }
+        unsigned long long late = 0ull;   // CTA 0's tmax decision, carried by its arrival
         if (tid == 0) {
             P.blk[b * 4 + 0] = part[0];
-            if (b == 0) {
-                const bool late = (double)(globaltimer_ns() - ctl->t_start_ns) * 1e-9 > ctl->tmax_s;
-                atomicExch(&P.bar->tmax_hit, late ? 1u : 0u);
-            }
+            if (b == 0 && (double)(globaltimer_ns() - ctl->t_start_ns) * 1e-9 > ctl->tmax_s) late = PERSIST_LATE;
         }
-        if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
+        if (!grid_sync(P.bar, gen, &sh.flag, late, &sh.late)) { failed = true; break; }
         // FIN_SK_ITER, the same in every CTA
         iter += 1;
         int pending = 0;
         if (iter >= itermax) pending = 2;
-        else if (ld_acquire_u32(&P.bar->tmax_hit)) pending = 3;
+        else if (sh.late) pending = 3;
         const bool do_check = ((iter - 1) % freq) == 0;
         if (!do_check) {
             num_iter += 1;
@@ -722,6 +728,7 @@ struct LShared {
     double fl[32], fe[32];     // the group's rows recomputed by the fallback
     unsigned bad;              // rows of the group outside the window
     int flag;
+    int late;                  // tmax passed (CTA 0's decision, via the barrier)
 };
 
 // Rows of one side for a pass with exponent coefficient a2 (log2 units):
@@ -938,18 +945,17 @@ __global__ void __launch_bounds__(PTPB, 1) lamp_persist_kernel(const __grid_cons
                                   sh.nu, sh.nub, sh.th, sh.thb, sh.emu, sh.ref[1]};
         pass_rows<PM, D, false, 4, false>(sy, sh.side[1], P.X, P.n, P.aux, LOG2E, ctr, a2n, inv_winf, P.pexp,
                                           eb, sh, part);
-        if (tid == 0 && b == 0) {
-            const bool late = (double)(globaltimer_ns() - ctl->t_start_ns) * 1e-9 > ctl->tmax_s;
-            atomicExch(&P.bar->tmax_hit, late ? 1u : 0u);
-        }
-        if (!grid_sync(P.bar, gen, &sh.flag)) { failed = true; break; }
+        unsigned long long late = 0ull;
+        if (tid == 0 && b == 0 && (double)(globaltimer_ns() - ctl->t_start_ns) * 1e-9 > ctl->tmax_s)
+            late = PERSIST_LATE;
+        if (!grid_sync(P.bar, gen, &sh.flag, late, &sh.late)) { failed = true; break; }
         // FIN_LAMP_B, the same in every CTA
         eta_t = eta_n;
         s_t = s_n;
         iter += 1;
         int pending = 0;
         if (iter >= itermax) pending = 2;
-        else if (ld_acquire_u32(&P.bar->tmax_hit)) pending = 3;
+        else if (sh.late) pending = 3;
         do_check = check_enabled && (iter % freq) == 0;
         if (pending) { stop_reason = pending; break; }
     }
