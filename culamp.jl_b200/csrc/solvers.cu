@@ -145,7 +145,9 @@ int ensure_solver(culamp_handle h, int n, int m, int d, int64_t log_cap, int fea
             return culamp_set_error(h, CULAMP_ERR_CUDA, "stream/event creation failed");
     }
     Solver &S = *h->solver;
-    const size_t nm = (size_t)(n > m ? n : m);
+    // + 2: the persistent loops copy column potentials in aligned pairs, which
+    // may reach one element past the last column
+    const size_t nm = (size_t)(n > m ? n : m) + 2;
     auto ptrs = [&S]() {
         return std::vector<void *>{S.X.ptr, S.Y.ptr, S.r.ptr, S.c.ptr, S.phi.ptr, S.psi.ptr,
                                    S.res.ptr, S.cost.ptr, S.logz.ptr, S.aux.ptr, S.nu.ptr,
