@@ -49,6 +49,7 @@ constexpr int PWARPS = PTPB / 32;
 constexpr int PRG = 28;                    // rows per group (warp 0 finishes one row per lane)
 constexpr int PMAXR = 56;                  // rows per CTA and side (2 groups)
 constexpr unsigned long long PERSIST_WAIT_NS = 2000000000ull;
+constexpr int PERSIST_CARVEOUT = 10;       // percent of the unified L1 / shared memory
 
 struct GridBar {
     // arrivals since the launch in the low 44 bits; + PERSIST_LATE once CTA 0
@@ -1019,26 +1020,30 @@ cudaError_t launch_pm(int d, const cudaLaunchConfig_t &cfg, const PersistParams 
 
 }  // namespace
 
-int persist_grid(int sm_count, int d, int pm) {
+// One CTA per SM, if the kernel fits; the shared-memory carveout is kept at
+// the least the kernel needs (~20 KB) so the rest of the SM's 256 KB serves as
+// L1 for the column loads.
+template <class FN>
+int persist_grid_of(FN fn, int sm_count) {
     int per_sm = 0;
-    cudaError_t e;
-    if (pm == P_SQ)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, d == 1 ? sk_persist_kernel<P_SQ, 1> : d == 2 ? sk_persist_kernel<P_SQ, 2> : sk_persist_kernel<P_SQ, 3>,
-            PTPB, 0);
-    else if (pm == P_L1)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, d == 1 ? sk_persist_kernel<P_L1, 1> : d == 2 ? sk_persist_kernel<P_L1, 2> : sk_persist_kernel<P_L1, 3>,
-            PTPB, 0);
-    else
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, d == 1 ? sk_persist_kernel<P_INF, 1> : d == 2 ? sk_persist_kernel<P_INF, 2> : sk_persist_kernel<P_INF, 3>,
-            PTPB, 0);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, PERSIST_CARVEOUT);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PTPB, 0);
     if (e != cudaSuccess || per_sm < 1) {
         cudaGetLastError();
         return 0;
     }
-    return sm_count;   // one CTA per SM
+    return sm_count;
+}
+
+int persist_grid(int sm_count, int d, int pm) {
+    if (pm == P_SQ)
+        return persist_grid_of(d == 1 ? sk_persist_kernel<P_SQ, 1> : d == 2 ? sk_persist_kernel<P_SQ, 2>
+                                                                          : sk_persist_kernel<P_SQ, 3>, sm_count);
+    if (pm == P_L1)
+        return persist_grid_of(d == 1 ? sk_persist_kernel<P_L1, 1> : d == 2 ? sk_persist_kernel<P_L1, 2>
+                                                                          : sk_persist_kernel<P_L1, 3>, sm_count);
+    return persist_grid_of(d == 1 ? sk_persist_kernel<P_INF, 1> : d == 2 ? sk_persist_kernel<P_INF, 2>
+                                                                       : sk_persist_kernel<P_INF, 3>, sm_count);
 }
 
 namespace {
@@ -1053,15 +1058,7 @@ LampFn lamp_fn(int d, int pm) {
 
 }  // namespace
 
-int lamp_persist_grid(int sm_count, int d, int pm) {
-    int per_sm = 0;
-    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lamp_fn(d, pm), PTPB, 0);
-    if (e != cudaSuccess || per_sm < 1) {
-        cudaGetLastError();
-        return 0;
-    }
-    return sm_count;
-}
+int lamp_persist_grid(int sm_count, int d, int pm) { return persist_grid_of(lamp_fn(d, pm), sm_count); }
 
 size_t lamp_persist_scratch_bytes(int grid) {
     return (size_t)grid * LAMP_SLOTS * sizeof(double) + sizeof(GridBar);
