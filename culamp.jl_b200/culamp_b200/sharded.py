@@ -30,7 +30,10 @@ iterations.
 A process may own several shards (its row blocks are reduced locally first),
 so the same driver runs one rank per GPU over NCCL, several row blocks on one
 GPU, or -- with compute ops that run on the host -- gloo ranks on CPU. Every
-rank issues the same collectives in the same order. tmax is tested on check
+rank issues the same collectives in the same order. With the CUDA ops the
+Sinkhorn driver captures the `frequency` iterations between two checks (the
+passes, the combines and the all_gather on the NCCL stream) in one CUDA graph
+and replays it, so the host takes part once per check. tmax is tested on check
 iterations (the reference tests it every iteration; a per-iteration test would
 need a collective per iteration to keep the ranks in step).
 """
@@ -111,10 +114,16 @@ def _reduce(t, op, group):
 
 
 def sharded_sinkhorn(x_shards, r_shards, y, c, args: EOTArgs, frequency: int = 100, p: float = 2.0,
-                     group=None, ops=None, phi0=None, psi0=None) -> ShardedResult:
+                     group=None, ops=None, phi0=None, psi0=None, graph: bool | None = None) -> ShardedResult:
     """Kernel Sinkhorn with the rows split over shards and ranks (see module doc).
     x_shards / r_shards: this rank's row blocks (same device); y, c: full.
-    Without an initialised process group the shards are those of one process."""
+    Without an initialised process group the shards are those of one process.
+
+    graph (default: on for the CUDA ops): the `frequency` iterations between
+    two checks -- passes, the combine and the all_gather -- are captured once
+    in a CUDA graph and replayed, so the host meets the device once per check
+    instead of once per pass; the first iteration runs eagerly (it warms the
+    kernels, the scratch and the communicator before the capture)."""
     ops = ops or CudaOps()
     if frequency < 1:
         raise ValueError("frequency must be >= 1")
@@ -146,7 +155,9 @@ def sharded_sinkhorn(x_shards, r_shards, y, c, args: EOTArgs, frequency: int = 1
             s[1] += cost
         return _reduce(s, dist.ReduceOp.SUM, group)
 
-    for it in range(1, args.itermax + 1):
+    def iterate():
+        # one iteration; phi and psi are updated in place (a captured graph
+        # replays on the same buffers)
         for x, r, ph in zip(x_shards, r_shards, phis):
             ops.lse_rows(ph, x, y, r, psi, eta, winf, ip)
         for x, ph, out in zip(x_shards, phis, outs):
@@ -154,9 +165,23 @@ def sharded_sinkhorn(x_shards, r_shards, y, c, args: EOTArgs, frequency: int = 1
         local = ops.combine(torch.stack(outs)) if len(outs) > 1 else outs[0]
         if world > 1:
             dist.all_gather(gathered, local.contiguous(), group=group)
-            psi = ops.combine(torch.stack(gathered))
+            psi.copy_(ops.combine(torch.stack(gathered)))
         else:
-            psi = local.clone()
+            psi.copy_(local)
+
+    use_graph = (isinstance(ops, CudaOps) if graph is None else graph) and y.is_cuda and frequency > 1
+    cg = None
+    it = 0
+    while it < args.itermax:
+        if cg is not None and it + frequency <= args.itermax:
+            # iterations it + 1 .. it + frequency: the last is the next check
+            # iteration ((it - 1) % frequency == 0 below); the others count here
+            cg.replay()
+            it += frequency
+            num_iter += frequency - 1
+        else:
+            iterate()
+            it += 1
         if (it - 1) % frequency == 0:
             s = resid()
             if float(s[0]) <= args.epsilon / 6.0:
@@ -168,6 +193,13 @@ def sharded_sinkhorn(x_shards, r_shards, y, c, args: EOTArgs, frequency: int = 1
                 stopped = 3
                 break
         num_iter += 1
+        if use_graph and cg is None and it == 1:
+            # record (not run) one block of `frequency` iterations
+            torch.cuda.synchronize()
+            cg = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(cg):
+                for _ in range(frequency):
+                    iterate()
     s = resid()
     return ShardedResult(phis, psi, float(s[0]), float(s[1]), it, num_iter, winf, stopped,
                          time.perf_counter() - t0)

@@ -148,3 +148,28 @@ dist.destroy_process_group()
     assert out.returncode == 0, out.stderr[-2000:]
     it, one_it, stopped = eval(out.stdout.strip().splitlines()[-1])
     assert it == one_it and stopped == 1
+
+
+@pytest.mark.parametrize("itermax,eps", [(57, 0.0), (5000, 6e-6)])
+def test_graph_replayed_blocks_equal_the_eager_loop(itermax, eps):
+    """The default loop captures the `frequency` iterations between checks in
+    one CUDA graph; it must give exactly what the eager loop gives (same
+    kernels on the same buffers): potentials bit for bit, counters, stop."""
+    import torch
+    import culamp_b200 as cb
+    from culamp_b200 import datasets as D
+    from culamp_b200.sharded import shard_rows, sharded_sinkhorn
+    x, y, r, c = D.grid_instance(24, 24, "mixture")
+    X, Y, R, Cc = (torch.as_tensor(v, device="cuda") for v in (x, y, r, c))
+    blocks = [shard_rows(x.shape[0], 3, k) for k in range(3)]
+    xs = [X[s:e].contiguous() for s, e in blocks]
+    rs = [R[s:e].contiguous() for s, e in blocks]
+    a = cb.EOTArgs(eta_p=1e-2, epsilon=eps, itermax=itermax, verbose=False)
+    g = sharded_sinkhorn(xs, rs, Y, Cc, a, frequency=10, p=2.0)
+    e = sharded_sinkhorn(xs, rs, Y, Cc, a, frequency=10, p=2.0, graph=False)
+    assert (g.iterations, g.num_iter, g.stopped) == (e.iterations, e.num_iter, e.stopped)
+    for pg, pe in zip(g.phi, e.phi):
+        assert torch.equal(pg, pe)
+    assert torch.equal(g.psi, e.psi)
+    if eps > 0:
+        assert g.stopped == 1
