@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--profile-persist", type=int, default=0, metavar="ITERS",
                     help="only run one ITERS-iteration Sinkhorn solve of the bench instance "
                          "(one sk_persist_kernel launch), for profiler captures")
+    ap.add_argument("--profile-solver", default="sinkhorn", choices=["sinkhorn", "lamp"],
+                    help="solver of the --profile-persist solve (lamp: one lamp_persist_kernel launch, "
+                         "checks every 10 iterations)")
     ap.add_argument("--profile-form", default="fp64", choices=["fp64", "fp32"],
                     help="exponent form of the --profile-pass solve")
     ap.add_argument("--profile-feature", type=int, default=0, metavar="N",
@@ -124,8 +127,11 @@ def profile_persist(args):
     if args.profile_steady and os.path.exists(args.profile_steady):
         z = np.load(args.profile_steady)
         kw = {"phi0": torch.as_tensor(z["phi"], device="cuda"), "psi0": torch.as_tensor(z["psi"], device="cuda")}
-    a = cb.EOTArgs(eta_p=ETA, epsilon=0.0, itermax=args.profile_persist, verbose=False)
-    res = cb.solve_sinkhorn(X, Y, R, Cc, a, FREQ, P, **kw)
+    a = cb.EOTArgs(eta_p=ETA, epsilon=0.0, itermax=args.profile_persist, verbose=False, B=1.1)
+    if args.profile_solver == "lamp":
+        res = cb.solve_lamp(X, Y, R, Cc, a, FREQ, P, flags=cb.FLAG_CHECK_ALWAYS)
+    else:
+        res = cb.solve_sinkhorn(X, Y, R, Cc, a, FREQ, P, **kw)
     torch.cuda.synchronize()
     print(json.dumps({"profile_persist": args.profile_persist, "iterations": res.iterations,
                       "loop_ms": res.elapsed_ms, "finite": bool(torch.isfinite(res.phi).all())}))
