@@ -587,7 +587,7 @@ def form_leg(cb, X, Y, R, C, freq, flags, chosen):
 
 
 def extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_chosen, chosen_ms):
-    """Chosen vs plain FP32 form, LAMP, and the 65536-point north-star solve."""
+    """Chosen vs plain FP32 form, LAMP, and the 65536-point solves."""
     ex = {}
     a = cb.EOTArgs(eta_p=ETA, epsilon=EPS, itermax=20 * it_chosen, tmax=60.0, verbose=False)
     t0 = time.perf_counter()
@@ -611,7 +611,7 @@ def extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_chosen, chosen_ms):
     ex["lamp_chosen"] = {"reached_tol": lr.stopped == 1, "ms": lr.elapsed_ms,
                          "wall_ms": (time.perf_counter() - t0) * 1e3,
                          "iterations": lr.iterations, "residual": lr.residual}
-    # north star: n = m = 65536 RGB clouds, eta 1e-3, Sinkhorn to 1e-6
+    # n = m = 65536 RGB clouds, eta 1e-3, Sinkhorn to 1e-6
     x5, y5, r5, c5 = D.rgb_instance(65536, 65536)
     X5, Y5, R5, C5 = (torch.as_tensor(v, device=dev) for v in (x5, y5, r5, c5))
     a5 = cb.EOTArgs(eta_p=ETA, epsilon=EPS, itermax=20000, tmax=60.0, verbose=False)

@@ -9,7 +9,7 @@ eta_p in {1e-3, 1e-4}.
 * Sinkhorn (SinkhornKernel.jl:477-559), LAMP (MirrorProxKernel.jl:1019-1132)
   and annealed Sinkhorn (AnnealedSinkhorn.jl:65-177) at a fixed iteration
   count: same iteration / num_iter counters, same convergence-log check
-  iterations, potentials within 1e-5 of max |potential|,
+  iterations, potentials within 1e-5 of max |potential| (the parity bar),
   objective within 1e-5 relative, LAMP's eta_t recursion bit-exact.
 * Stopping rules: the Sinkhorn solve to 1e-6 L1 (eta_p = 1e-3, p = 2, check
   every 10) stops at the oracle's own iteration; LAMP with its full rule

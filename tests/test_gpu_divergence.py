@@ -5,7 +5,7 @@
 * The divergence gradient against central finite differences of FP64 oracle
   solves: h = 1e-3 on 64 coordinates at eta_p = 1e-2 (n = 256), and h = 2e-4
   on 12 coordinates at the divergence workload's eta_p = 1e-3 (n = 1024):
-  1e-4 relative. eps is held fixed across the perturbed
+  1e-4 relative (the gradient parity bar). eps is held fixed across the perturbed
   solves.
 """
 import math

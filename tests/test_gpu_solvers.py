@@ -2,7 +2,7 @@
 committed golden fixtures: same iteration counts / stopping iteration, same
 convergence-log rows, potentials and objectives within tolerance.
 
-Potentials are compared two ways. (1) Raw, at the north-star bar: max error
+Potentials are compared two ways. (1) Raw, at the 1e-5 parity bar: max error
 <= 1e-5 of max |potential|. (2) Gauge-fixed (the r-weighted mean removed), at
 5e-6 absolute for Sinkhorn: Sinkhorn's plan exp(phi_i + psi_j - C/eps) is
 invariant to phi + k, psi - k, and LAMP's to a uniform shift of nu, and those
