@@ -94,7 +94,7 @@ __device__ __forceinline__ void red_release_add_u64(unsigned long long *p, unsig
 // Returns false (in every thread of the CTA) when this CTA gave up or saw
 // another CTA give up.
 __device__ bool grid_sync(GridBar *gb, unsigned &gen, int *s_flag, unsigned long long extra = 0ull,
-                          int *s_late = nullptr) {
+                          int *s_late = nullptr, unsigned long long limit_ns = PERSIST_WAIT_NS) {
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
@@ -111,7 +111,7 @@ __device__ bool grid_sync(GridBar *gb, unsigned &gen, int *s_flag, unsigned long
             if ((spins & 63u) == 63u) {
                 const unsigned long long t = globaltimer_ns();
                 if (t0 == 0) t0 = t;
-                else if (t - t0 > PERSIST_WAIT_NS) {
+                else if (t - t0 > limit_ns) {
                     red_release_add_u64(&gb->count, PERSIST_ABORT);
                     ok = 0;
                     break;
@@ -986,6 +986,20 @@ __global__ void __launch_bounds__(PTPB, 1) lamp_persist_kernel(const __grid_cons
     (void)SQ;
 }
 
+// The grid barrier on a barrier that one CTA never reaches: CTA 1 leaves at
+// once, CTA 0 waits with the given limit. out = {CTA 0's wait gave up, the
+// counter carries PERSIST_ABORT}.
+__global__ void grid_wait_probe_kernel(GridBar *gb, unsigned long long limit_ns, int *out) {
+    __shared__ int flag;
+    if (blockIdx.x != 0) return;
+    unsigned gen = 0;
+    const bool ok = grid_sync(gb, gen, &flag, 0ull, nullptr, limit_ns);
+    if (threadIdx.x == 0) {
+        out[0] = ok ? 0 : 1;
+        out[1] = (gb->count >= PERSIST_ABORT) ? 1 : 0;
+    }
+}
+
 }  // namespace culamp_dev
 
 
@@ -1115,3 +1129,37 @@ cudaError_t launch_sk_persist(const double *X, const double *Y, const double *r,
 }
 
 }  // namespace culamp_host
+
+extern "C" int culamp_probe_grid_wait(culamp_handle h, uint64_t limit_ns, void *stream) {
+    using namespace culamp_dev;
+    if (!h) return CULAMP_ERR_INVALID_ARG;
+    if (limit_ns == 0 || limit_ns > 10000000000ull)
+        return culamp_set_error(h, CULAMP_ERR_INVALID_ARG, "wait limit must be in (0, 10 s]");
+    cudaSetDevice(h->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (h->tmpA.reserve(sizeof(GridBar) + 2 * sizeof(int)) != cudaSuccess)
+        return culamp_set_error(h, CULAMP_ERR_ALLOC, "probe buffer");
+    GridBar *gb = h->tmpA.as<GridBar>();
+    int *dev = reinterpret_cast<int *>(gb + 1);
+    if (cudaMemsetAsync(h->tmpA.ptr, 0, sizeof(GridBar) + 2 * sizeof(int), st) != cudaSuccess)
+        return culamp_set_error(h, CULAMP_ERR_CUDA, "probe set-up failed");
+    // two co-resident CTAs, as the persistent loops launch theirs
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2);
+    cfg.blockDim = dim3(32);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int out[2] = {-1, -1};
+    if (cudaLaunchKernelEx(&cfg, grid_wait_probe_kernel, gb, (unsigned long long)limit_ns, dev) != cudaSuccess ||
+        cudaMemcpyAsync(out, dev, sizeof(out), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return culamp_set_error(h, CULAMP_ERR_CUDA, "grid wait probe failed");
+    if (out[0] == 1 && out[1] == 1)
+        return culamp_set_error(h, CULAMP_ERR_DEVICE_TIMEOUT, "grid barrier wait gave up after %llu ns",
+                                (unsigned long long)limit_ns);
+    return culamp_set_error(h, CULAMP_ERR_CUDA, "grid barrier wait did not give up (%d, %d)", out[0], out[1]);
+}

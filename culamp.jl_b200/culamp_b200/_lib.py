@@ -127,6 +127,7 @@ SIGNATURES = {
                                    C.POINTER(CLogRow), _I64]),
     "culamp_probe_pipes": (C.c_int, [_VP, C.POINTER(_D), _VP]),
     "culamp_probe_wait": (C.c_int, [_VP, C.c_uint64, _VP]),
+    "culamp_probe_grid_wait": (C.c_int, [_VP, C.c_uint64, _VP]),
     "culamp_adjoint_sk": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, _D, _D, _D,
                                     _VP]),
     "culamp_lse_rows_sk_noalloc": (C.c_int, [_VP, _VP, _VP, _I64, _I64, _I32, _VP, _VP, _D, _D, _D,

@@ -397,6 +397,13 @@ int culamp_probe_pipes(culamp_handle h, double *out, void *stream);
  * it must; the device context stays usable. Synchronous. */
 int culamp_probe_wait(culamp_handle h, uint64_t limit_ns, void *stream);
 
+/* No counterpart in the reference. Runs the persistent loops' grid barrier
+ * (two co-resident CTAs, one of which never arrives) with the given wait limit
+ * in ns (at most 10 s). Returns CULAMP_ERR_DEVICE_TIMEOUT when the waiting CTA
+ * gave up and published the abort, as it must; the device context stays
+ * usable. Synchronous. */
+int culamp_probe_grid_wait(culamp_handle h, uint64_t limit_ns, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
