@@ -23,18 +23,20 @@
 //     scaled by 2^FR_C0). Rows whose sums leave the window are shared out to
 //     the CTA's warps and recomputed without a reference (a max pass, then a
 //     sum pass of max-shifted terms).
-//   * Half-steps are separated by a grid barrier (one arrival counter and one
-//     generation word in global memory). Every wait on it is bounded: after
-//     PERSIST_WAIT_NS a waiting CTA sets the abort word and the control block's
-//     error flag and every CTA leaves the loop; the host reports a device
-//     timeout.
+//   * Half-steps are separated by a grid barrier (one monotonic arrival
+//     counter in global memory). Every wait on it is bounded: after
+//     PERSIST_WAIT_NS a waiting CTA adds the abort mark to the counter, sets
+//     the control block's error flag and every CTA leaves the loop; the host
+//     reports a device timeout.
 //   * The control step of each iteration (iteration counter, check cadence,
 //     itermax, tmax, the tolerance test of the check iterations) follows the
 //     pass engine's FIN_SK_ITER / FIN_SK_CHECK. Decisions that every CTA needs
 //     are computed by every CTA from the same data in the same order (the
-//     tolerance test sums the per-CTA partials in CTA order); the one decision
-//     that reads the clock (tmax) is taken by CTA 0 and published before it
-//     arrives at the barrier. CTA 0 alone writes the control block and the log.
+//     tolerance test sums the per-CTA partials in a fixed order); the one
+//     decision that reads the clock (tmax) is taken by CTA 0 and carried by its
+//     arrival at the barrier. CTA 0 alone writes the control block and the log.
+//
+// The same machinery runs LAMP's loop (lamp_persist_kernel, further below).
 //
 // Potentials written by other CTAs are read with L2-coherent loads (ld.cg).
 
@@ -823,7 +825,6 @@ __global__ void __launch_bounds__(PTPB, 1) lamp_persist_kernel(const __grid_cons
     __shared__ double s_tot[LAMP_SLOTS];
     __shared__ double s_chk[4];     // residual, cost, primal, dual of the last check
     __shared__ int s_stop;
-    constexpr bool SQ = (PM == P_SQ);
     Ctl *ctl = P.ctl;
     if (ctl->stop) return;
     const double winf = ctl->winf, eta_l = ctl->eta_lamp, tau_p = ctl->tau_p, hr = ctl->hr;
@@ -983,7 +984,6 @@ __global__ void __launch_bounds__(PTPB, 1) lamp_persist_kernel(const __grid_cons
         ctl->primal = s_chk[2];
         ctl->dual = s_chk[3];
     }
-    (void)SQ;
 }
 
 // The grid barrier on a barrier that one CTA never reaches: CTA 1 leaves at
