@@ -608,7 +608,8 @@ def extras(cb, K, D, torch, np, X, Y, R, Cc, dev, it_chosen, chosen_ms):
     cb.solve_lamp(X, Y, R, Cc, b.copy(itermax=50), FREQ, P, flags=fl)
     t0 = time.perf_counter()
     lr = cb.solve_lamp(X, Y, R, Cc, b, FREQ, P, flags=fl)
-    ex["lamp_chosen"] = {"reached_tol": lr.stopped == 1, "ms": lr.elapsed_ms,
+    ex["lamp_chosen"] = {"form": "persistent loop, FP64 exponent", "reached_tol": lr.stopped == 1,
+                         "ms": lr.elapsed_ms,
                          "wall_ms": (time.perf_counter() - t0) * 1e3,
                          "iterations": lr.iterations, "residual": lr.residual}
     # n = m = 65536 RGB clouds, eta 1e-3, Sinkhorn to 1e-6
