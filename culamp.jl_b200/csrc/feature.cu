@@ -118,7 +118,7 @@ __device__ __noinline__ bool ft_wait(uint32_t bar, uint32_t parity, volatile int
     }
 }
 
-// Lane 0 waits, the warp follows its verdict.
+// Lane 0 waits; the whole warp takes its result (phase reached, or gave up).
 __device__ __forceinline__ bool warp_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag) {
     bool ok = true;
     if ((threadIdx.x & 31) == 0) ok = ft_wait(bar, parity, abort_flag, true);
