@@ -560,7 +560,7 @@ extern "C" int culamp_batched_sinkhorn(culamp_handle h, const culamp_instance *i
         sig.push_back(((unsigned long long)I.n << 40) ^ ((unsigned long long)I.m << 12) ^ (unsigned long long)I.d);
     }
     const int sms = h->sm_count;
-    const std::vector<int> tpsms = {2, 4, 8, 16, 32};
+    const std::vector<int> tpsms = {2, 4, 8, 16, 32, 64};
     const std::vector<int> tpus = {4, 16};
     size_t parto = 0, ticko = 0, blko = 0;
     for (Inst &I : X.in) {
@@ -650,8 +650,9 @@ extern "C" int culamp_batched_sinkhorn(culamp_handle h, const culamp_instance *i
         // later phases run fewer instances, and there more CTAs per SM keep the
         // GPU busier. Among candidates within TUNE_SLACK of the fastest, take
         // the one with the most CTAs per SM (measured on 512 uneven instances:
-        // 2, 4, 8, 16, 32 CTAs per SM -> 617, 605, 591-599, 574-581, 568 ms per
-        // solve, all within noise of each other in the tuning iterations).
+        // 2, 4, 8, 16, 32, 64 CTAs per SM -> 617, 605, 591-599, 574-581, 568,
+        // 536 ms per solve, all within noise of each other in the tuning
+        // iterations; 128 gave 535 ms for more tuning time).
         constexpr float TUNE_SLACK = 1.03f;
         float pick = 1e30f;
         tpsm = 0;
